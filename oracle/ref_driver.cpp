@@ -1,0 +1,198 @@
+// Oracle driver around the reference SQDFT objects (test infrastructure).
+//
+// Runs the reference's own set-up for an input stem exactly as main.cpp:30-106
+// and SQDFT_forces (scf.cpp:341-372) do up to the first SQ call, then calls
+// the reference's ClenshawCurtisSpectralQuadrature (sq.cpp:377),
+// HsubTimesVec (sq.cpp:838) and ForcesNonLocal (forces.cpp:318), and writes
+// their inputs and outputs as case containers (sqdft_b200/csrc/sq_case.h).
+//
+// usage: sqref_driver <run_dir> <stem> <out_prefix> [options]
+//   --veff FILE      replace the Veff block interior (np_z*np_y*np_x float64,
+//                    z-major) before the SQ call
+//   --scf-iter K     scf_iter passed to the SQ call (default 1)
+//   --lambda-f X     warm-start Fermi level used when K > 1
+//   --no-forces      skip ForcesNonLocal
+//   --hv K           also apply HsubTimesVec to K seeded vectors at K nodes
+//   --nodes-only     stop after the SQ set-up (export the inputs only)
+// Writes <out_prefix>_in.sqc (inputs, incl. the reference's UdVtm tables) and
+// <out_prefix>_out.sqc (outputs and timings).
+#include <unistd.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ds_sq.h"
+#include "func_sq.h"
+#include "../sqdft_b200/dropin/sq_export.h"
+
+static unsigned long long lcg_state = 0x9E3779B97F4A7C15ull;
+static double lcg_uniform() {  // deterministic [-1, 1) values for the HsubTimesVec fixture
+  lcg_state = lcg_state * 6364136223846793005ull + 1442695040888963407ull;
+  return ((double)(lcg_state >> 11) / 9007199254740992.0) * 2.0 - 1.0;
+}
+
+int main(int argc, char **argv) {
+  if (argc < 4) {
+    std::fprintf(stderr, "usage: %s run_dir stem out_prefix [options]\n", argv[0]);
+    return 2;
+  }
+  std::string run_dir = argv[1], stem = argv[2], out = argv[3];
+  std::string veff_file;
+  int scf_iter = 1, hv_count = 0, do_forces = 1, nodes_only = 0;
+  double lambda_warm = 0.0;
+  int have_lambda = 0;
+  for (int a = 4; a < argc; a++) {
+    if (!std::strcmp(argv[a], "--veff") && a + 1 < argc) veff_file = argv[++a];
+    else if (!std::strcmp(argv[a], "--scf-iter") && a + 1 < argc) scf_iter = std::atoi(argv[++a]);
+    else if (!std::strcmp(argv[a], "--lambda-f") && a + 1 < argc) { lambda_warm = std::atof(argv[++a]); have_lambda = 1; }
+    else if (!std::strcmp(argv[a], "--no-forces")) do_forces = 0;
+    else if (!std::strcmp(argv[a], "--hv") && a + 1 < argc) hv_count = std::atoi(argv[++a]);
+    else if (!std::strcmp(argv[a], "--nodes-only")) nodes_only = 1;
+    else { std::fprintf(stderr, "unknown option %s\n", argv[a]); return 2; }
+  }
+  // Output paths are made absolute before changing into the run directory.
+  if (out[0] != '/') {
+    char cwd[4096];
+    if (getcwd(cwd, sizeof(cwd))) out = std::string(cwd) + "/" + out;
+  }
+  if (chdir(run_dir.c_str()) != 0) { std::perror("chdir"); return 2; }
+
+  DS_SQ SQ = {};
+  MPI_Init(&argc, &argv);
+  SQ.nproc = 1;
+  // CheckInputs reads the stem from the bytes after "-name" (readfiles.cpp:72-80).
+  std::string argblob = std::string("-name") + '\0' + stem + '\0';
+  std::vector<char> blob(argblob.begin(), argblob.end());
+  char *fake_argv[3] = {argv[0], blob.data(), blob.data() + 6};
+  CheckInputs(&SQ, fake_argv);
+  SQ.mpi_time = 0.0;
+  Read_input(&SQ);
+  Read_atoms(&SQ);
+  Read_psd(&SQ);
+  Processor_domain(&SQ);
+  AllocateArrays(&SQ);
+  Comm_topologies(&SQ);
+  Laplacian_Comm_Indices(&SQ);
+  SQ_Comm_Indices(&SQ);
+  SQ.MDstepCount = 1;
+
+  Replica_atoms(&SQ);
+  ChargeDensity(&SQ);
+  if (SQ.Correction == 2) OverlapCorrection(&SQ);
+  Replica_atoms_Rcut(&SQ);
+  double t0 = MPI_Wtime();
+  NonlocalProjectors(&SQ);
+  double t_proj = MPI_Wtime() - t0;
+  PoissonSolver_AAJ(&SQ);
+  ExchangeCorrelationPotential(&SQ);
+  EvaluateEffectivePotential(&SQ);
+
+  const int nl = SQ.nloc, nx = SQ.np_x, ny = SQ.np_y, nz = SQ.np_z;
+  const int nnode = nx * ny * nz;
+  if (!veff_file.empty()) {
+    std::vector<double> vb((size_t)nnode);
+    FILE *f = std::fopen(veff_file.c_str(), "rb");
+    if (!f || std::fread(vb.data(), sizeof(double), vb.size(), f) != vb.size()) {
+      std::fprintf(stderr, "cannot read %s\n", veff_file.c_str());
+      return 2;
+    }
+    std::fclose(f);
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) SQ.Veff[k + nl][j + nl][i + nl] = vb[((size_t)k * ny + j) * nx + i];
+  }
+  if (have_lambda) SQ.lambda_f = lambda_warm;
+  const double lambda_in = SQ.lambda_f;
+
+  if (nodes_only) {
+    // Only the block interior is valid here; the SQ call fills the halo.
+    sqb::export_case(&SQ, (out + "_in.sqc").c_str(), scf_iter, true);
+    return 0;
+  }
+
+  t0 = MPI_Wtime();
+  ClenshawCurtisSpectralQuadrature(&SQ, scf_iter);
+  const double t_sq = MPI_Wtime() - t0;
+  const double lambda_out = SQ.lambda_f;
+
+  // Inputs: the SQ call filled the Veff halo by its own exchange; the warm
+  // start is the value the call began with.
+  SQ.lambda_f = lambda_in;
+  sqb::export_case(&SQ, (out + "_in.sqc").c_str(), scf_iter, true);
+  SQ.lambda_f = lambda_out;
+
+  sqb::CaseWriter w(out + "_out.sqc");
+  std::vector<double> rho((size_t)nnode), rpj((size_t)nnode * (SQ.npl + 1)), ci((size_t)nnode * (SQ.npl + 1));
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) rho[((size_t)k * ny + j) * nx + i] = SQ.rho[k][j][i];
+  for (int n = 0; n < nnode; n++)
+    for (int q = 0; q <= SQ.npl; q++) {
+      rpj[(size_t)n * (SQ.npl + 1) + q] = SQ.rho_pj[n][q];
+      ci[(size_t)n * (SQ.npl + 1) + q] = SQ.Ci[n][q];
+    }
+  w.f64("rho", rho.data(), {nz, ny, nx});
+  w.f64("rho_pj", rpj.data(), {nnode, SQ.npl + 1});
+  w.f64("Ci", ci.data(), {nnode, SQ.npl + 1});
+  w.f64("chi", SQ.chi, {nnode});
+  w.f64("zee", SQ.zee, {nnode});
+  w.f64s("lambda_f", lambda_out);
+  w.f64s("Ebs", SQ.Ebs);
+  w.f64s("Eent", SQ.Eent);
+  w.f64s("t_sq", t_sq);
+  w.f64s("t_projectors", t_proj);
+
+  if (hv_count > 0) {
+    const int n = 2 * nl + 1;
+    const size_t nw = (size_t)n * n * n;
+    std::vector<int> nodes;
+    std::vector<double> vin, vout;
+    double ***vec = new double **[n], ***hv = new double **[n];
+    for (int k = 0; k < n; k++) {
+      vec[k] = new double *[n];
+      hv[k] = new double *[n];
+      for (int j = 0; j < n; j++) {
+        vec[k][j] = new double[n];
+        hv[k][j] = new double[n];
+      }
+    }
+    for (int c = 0; c < hv_count; c++) {
+      const int node = (int)(((long long)c * 7919 + 13) % nnode);
+      const int i = node % nx, j = (node / nx) % ny, k = node / (nx * ny);
+      nodes.push_back(node);
+      for (int kk = 0; kk < n; kk++)
+        for (int jj = 0; jj < n; jj++)
+          for (int ii = 0; ii < n; ii++) {
+            vec[kk][jj][ii] = lcg_uniform();
+            vin.push_back(vec[kk][jj][ii]);
+          }
+      HsubTimesVec(&SQ, vec, i + nl, j + nl, k + nl, hv);
+      for (int kk = 0; kk < n; kk++)
+        for (int jj = 0; jj < n; jj++)
+          for (int ii = 0; ii < n; ii++) vout.push_back(hv[kk][jj][ii]);
+    }
+    w.i32("hv_nodes", nodes.data(), {hv_count});
+    w.f64("hv_in", vin.data(), {hv_count, (int64_t)nw});
+    w.f64("hv_out", vout.data(), {hv_count, (int64_t)nw});
+  }
+
+  if (do_forces) {
+    t0 = MPI_Wtime();
+    ForcesNonLocal(&SQ);
+    const double t_f = MPI_Wtime() - t0;
+    std::vector<double> f((size_t)SQ.n_atm * 3);
+    for (int a = 0; a < SQ.n_atm; a++) {
+      f[3 * a] = SQ.fnlocx[a];
+      f[3 * a + 1] = SQ.fnlocy[a];
+      f[3 * a + 2] = SQ.fnlocz[a];
+    }
+    w.f64("fnloc", f.data(), {SQ.n_atm, 3});
+    w.f64s("t_forces", t_f);
+  }
+  w.close();
+  std::printf("sqref_driver: wrote %s_in.sqc and %s_out.sqc (SQ %.3f s)\n", out.c_str(), out.c_str(), t_sq);
+  return 0;
+}

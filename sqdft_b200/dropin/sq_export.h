@@ -1,0 +1,106 @@
+// Serialise the SQ-step inputs held in a DS_SQ into a case container.
+//
+// Compiled against the reference headers (ds_sq.h, func_sq.h).  It reads the
+// fields that ClenshawCurtisSpectralQuadrature (sq.cpp:377-834),
+// NonlocalProjectors (nonlocal.cpp:317-518) and ForcesNonLocal
+// (forces.cpp:318-578) read, in the layouts ds_sq.h gives them:
+//   * Veff on the processor + Rcut block, [np_z+2nloc][np_y+2nloc][np_x+2nloc]
+//     (initialize.cpp:940-967), halo already filled;
+//   * replica atoms whose rc-ball meets the processor + Rcut block
+//     (Replica_atoms_Rcut, initialize.cpp:1003-1196), type-major, main atoms
+//     in input order, replicas in the reference's z-y-x image order;
+//   * per type the radial tables and spline derivatives (ds_sq.h:76-102) and
+//     the Kleinman-Bylander denominators (readfiles.cpp:1154-1216).
+#pragma once
+#include <cmath>
+#include <vector>
+
+#include "sq_case.h"
+
+namespace sqb {
+
+inline int proj_count(const DS_SQ *p, int t) {
+  int n = 0;
+  for (int l = 0; l <= p->Psd[t].lmax; l++)
+    if (l != p->Atm[t].lloc) n += 2 * l + 1;
+  return n;
+}
+
+inline void export_case(DS_SQ *p, const char *path, int scf_iter, bool with_udvtm) {
+  CaseWriter w(path);
+  const int nl = p->nloc;
+  const int ex = p->np_x + 2 * nl, ey = p->np_y + 2 * nl, ez = p->np_z + 2 * nl;
+  int pi[17] = {p->n_int[0], p->n_int[1], p->n_int[2], p->np_x, p->np_y, p->np_z,
+                p->pnode_s[0], p->pnode_s[1], p->pnode_s[2], p->nloc, p->FDn, p->npl,
+                p->fermi_alg, p->n_typ, p->n_atm, scf_iter, p->nproc};
+  w.i32("params_i", pi, {17});
+  double pd[8] = {p->delta, p->bet, p->lanczos_tol, p->fermi_tol, p->Ncharge, p->lambda_f, p->T, p->Rcut};
+  w.f64("params_d", pd, {8});
+  w.f64("coeff_lap", p->coeff_lap, {p->FDn + 1});
+  w.f64("coeff_grad", p->coeff_grad, {p->FDn + 1});
+
+  std::vector<double> v((size_t)ex * ey * ez);
+  for (int k = 0; k < ez; k++)
+    for (int j = 0; j < ey; j++)
+      for (int i = 0; i < ex; i++) v[((size_t)k * ey + j) * ex + i] = p->Veff[k][j][i];
+  w.f64("veff", v.data(), {ez, ey, ex});
+
+  std::vector<int> ti;
+  std::vector<double> td;
+  std::vector<int> ri;
+  std::vector<double> rx;
+  std::vector<double> ud;
+  std::vector<double> axyz;
+  std::vector<int> atyp;
+  int atom_count = 0;
+  for (int t = 0; t < p->n_typ; t++) {
+    const DS_Psd &ps = p->Psd[t];
+    const int nlocc = (int)ceil(ps.rc / p->delta);  // nonlocal.cpp:43
+    const int nproj = proj_count(p, t);
+    const int nnd = (2 * nlocc + 1) * (2 * nlocc + 1) * (2 * nlocc + 1);
+    int row[6] = {p->Atm[t].natm, ps.lmax, p->Atm[t].lloc, nlocc, ps.size, nproj};
+    ti.insert(ti.end(), row, row + 6);
+    double drow[6] = {ps.rc, ps.Denom_s, ps.Denom_p, ps.Denom_d, ps.Denom_f, (double)p->Atm[t].Z};
+    td.insert(td.end(), drow, drow + 6);
+
+    const double *tabs[19] = {ps.RadialGrid, ps.rVloc, ps.rVs, ps.rVp, ps.rVd, ps.rVf, ps.rUs,
+                              ps.rUp, ps.rUd, ps.rUf, ps.DVloc, ps.DVsJ, ps.DVpJ, ps.DVdJ,
+                              ps.DVfJ, ps.DUsJ, ps.DUpJ, ps.DUdJ, ps.DUfJ};
+    std::vector<double> st((size_t)19 * ps.size, 0.0);
+    for (int q = 0; q < 19; q++)
+      if (tabs[q])
+        for (int r = 0; r < ps.size; r++) st[(size_t)q * ps.size + r] = tabs[q][r];
+    char nm[32];
+    std::snprintf(nm, sizeof(nm), "psd%d", t);
+    w.f64(nm, st.data(), {19, ps.size});
+
+    for (int a = 0; a < p->Atm[t].natm; a++, atom_count++) {
+      axyz.push_back(p->Atm[t].Rx[a].main_atm);
+      axyz.push_back(p->Atm[t].Ry[a].main_atm);
+      axyz.push_back(p->Atm[t].Rz[a].main_atm);
+      atyp.push_back(t);
+      for (int r = 0; r < p->Atm[t].Rx[a].n_replica_Rcut; r++) {
+        int rr[3] = {t, a, atom_count};
+        ri.insert(ri.end(), rr, rr + 3);
+        rx.push_back(p->Atm[t].Rx[a].ProcAtmRcut[r].coord);
+        rx.push_back(p->Atm[t].Ry[a].ProcAtmRcut[r].coord);
+        rx.push_back(p->Atm[t].Rz[a].ProcAtmRcut[r].coord);
+        if (with_udvtm && p->Atm[t].Rx[a].ProcAtmRcut[r].UdVtm)
+          for (int c = 0; c < nproj; c++)
+            ud.insert(ud.end(), p->Atm[t].Rx[a].ProcAtmRcut[r].UdVtm[c],
+                      p->Atm[t].Rx[a].ProcAtmRcut[r].UdVtm[c] + nnd);
+      }
+    }
+  }
+  w.i32("typ_i", ti.data(), {p->n_typ, 6});
+  w.f64("typ_d", td.data(), {p->n_typ, 6});
+  const int64_t nrep = (int64_t)ri.size() / 3;
+  w.i32("rep_i", ri.data(), {nrep, 3});
+  w.f64("rep_xyz", rx.data(), {nrep, 3});
+  w.f64("atoms_xyz", axyz.data(), {(int64_t)atyp.size(), 3});
+  w.i32("atom_type", atyp.data(), {(int64_t)atyp.size()});
+  if (with_udvtm) w.f64("udvtm", ud.data(), {(int64_t)ud.size()});
+  w.close();
+}
+
+}  // namespace sqb
