@@ -1,0 +1,170 @@
+/* sqdft_b200: B200 (sm_100a) implementation of SQDFT's spectral-quadrature
+ * density / energy / nonlocal-force step, behind a C ABI.
+ *
+ * One context (sqb_ctx) holds one processor block of the SQDFT grid -- the
+ * whole periodic domain on a single GPU -- with its Veff, atoms and projector
+ * tables resident in HBM.  Every entry point replaces one reference function
+ * (cited as file:line of the SQDFT sources) and keeps its argument meaning;
+ * arrays are plain host pointers in the reference's own layouts:
+ *   node nd = (k*np_y + j)*np_x + i            (sq.cpp:530-535)
+ *   rho      [np_z][np_y][np_x]                 (DS_SQ::rho)
+ *   rho_pj, Ci [nnode][npl+1]                   (DS_SQ::rho_pj, DS_SQ::Ci)
+ *   chi, zee [nnode]                            (DS_SQ::chi, DS_SQ::zee)
+ *   veff     [np_z+2nloc][np_y+2nloc][np_x+2nloc], halo filled
+ *                                               (DS_SQ::Veff, initialize.cpp:940)
+ *   forces   [n_atm][3], atoms type-major       (fnlocx/y/z, forces.cpp:504-527)
+ * All functions return SQB_OK (0) or one of the SQB_ERR_* codes; none of them
+ * exits the process.  A context is used by one host thread at a time.
+ */
+#ifndef SQDFT_B200_H
+#define SQDFT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference prints and exit(1)s in the cases marked. */
+#define SQB_OK 0
+#define SQB_ERR_ARG 1              /* bad argument or size */
+#define SQB_ERR_CUDA 2             /* CUDA runtime error or no device */
+#define SQB_ERR_UNSUPPORTED 3      /* configuration outside what the kernels cover */
+#define SQB_ERR_NOT_BRACKETED 4    /* sq.cpp:1307-1311, Brent root not bracketed */
+#define SQB_ERR_FERMI_MAXITER 5    /* sq.cpp:1400-1401, Brent iteration limit */
+#define SQB_ERR_NEGATIVE_RHO 6     /* sq.cpp:764-765, rho < -1e-6 */
+#define SQB_ERR_LANCZOS_MAXITER 7  /* sq.cpp:1073-1074, Lanczos hit 500 iterations */
+#define SQB_ERR_DENOM_ZERO 8       /* nonlocal.cpp:163, zero KB denominator */
+#define SQB_ERR_SPLINE_RANGE 9     /* spline.cpp:17-22, radius outside the radial grid */
+#define SQB_ERR_CAPACITY 10        /* more projector atoms in one window than supported */
+#define SQB_ERR_NONFINITE 11       /* NaN or Inf met in inputs or in a result */
+#define SQB_ERR_STATE 12           /* entry point called before its inputs were set */
+
+/* Arithmetic of the recursion vectors (Chebyshev and Lanczos). */
+#define SQB_FP64 0        /* everything in FP64: parity path */
+#define SQB_FP32_MIXED 1  /* FP32 Chebyshev vectors and stencil, FP64 moments,
+                             Lanczos bounds, coefficients, Fermi solve, assembly */
+
+typedef struct sqb_ctx sqb_ctx;
+
+/* Grid and SQ parameters: the DS_SQ fields of ds_sq.h:133-161. */
+typedef struct sqb_grid {
+  int np[3];      /* np_x, np_y, np_z: nodes of this block */
+  int pnode_s[3]; /* global index of the block's first node */
+  int n_int[3];   /* global grid intervals (periodic) */
+  int nloc;       /* ceil(Rcut/delta), readfiles.cpp:306 */
+  int fdn;        /* half FD order; the kernels support 6 (12th order) */
+  int npl;        /* Chebyshev degree, multiple of 4 (sq.cpp:523) */
+  int fermi_alg;  /* 1 Brent, 2 Newton-Raphson */
+  double delta, bet, lanczos_tol, fermi_tol, ncharge;
+  double coeff_lap[8];  /* coeff_lap[0..fdn], readfiles.cpp:371-381 */
+  double coeff_grad[8]; /* coeff_grad[0..fdn], readfiles.cpp:384-389 */
+} sqb_grid;
+
+/* One atom type: DS_Psd (ds_sq.h:76-102) + DS_Atm fields. */
+typedef struct sqb_species {
+  int natm, lmax, lloc;
+  int nlocc;       /* ceil(rc/delta), nonlocal.cpp:43 */
+  int size;        /* radial grid length */
+  double rc;
+  double denom[4]; /* Denom_s, Denom_p, Denom_d, Denom_f */
+  /* 19 x size rows: RadialGrid, rVloc, rVs, rVp, rVd, rVf, rUs, rUp, rUd, rUf,
+   * DVloc, DVsJ, DVpJ, DVdJ, DVfJ, DUsJ, DUpJ, DUdJ, DUfJ; may be NULL when the
+   * projector tables are supplied by sqb_set_projectors. */
+  const double *tables;
+} sqb_species;
+
+/* Reduction operators of the allreduce hook. */
+#define SQB_SUM 0
+#define SQB_MIN 1
+#define SQB_MAX 2
+
+/* Reduce `count` doubles across ranks in place: MPI_Allreduce with MPI_SUM
+ * in the reference (sq.cpp:1219, 1442, 792; forces.cpp:623) and the
+ * MPI_Allgather + min/max of the Lanczos bounds (sq.cpp:676-713).  Return 0
+ * on success.  Unset means a single rank. */
+typedef int (*sqb_allreduce_fn)(double *values, int count, int op, void *user);
+
+/* Timings and counters of the last calls (CUDA events on the context's
+ * stream, milliseconds). */
+typedef struct sqb_stats {
+  double ms_lanczos_moments; /* node kernel of the last SQ call */
+  double ms_fermi;           /* Fermi-level solve */
+  double ms_density;         /* density / energy assembly */
+  double ms_forces;          /* nonlocal-force kernel + reduction */
+  double ms_projectors;      /* projector tables */
+  long long matvecs;         /* window matvecs in the last node kernel */
+  long long lanczos_iters;   /* sum of Lanczos iterations over nodes */
+  long long window_points;   /* (2nloc+1)^3 */
+  long long proj_points;     /* sum over nodes and matvecs of projector-ball points read (algorithmic) */
+  int fermi_iters;
+  int max_lanczos_iters;
+  int kernel_launches;       /* kernels launched by the last SQ or forces call */
+} sqb_stats;
+
+/* Create a context on CUDA device `device` (cudaSetDevice).  Mirrors the
+ * per-call allocations of sq.cpp:496-517 with resident device buffers. */
+int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out);
+int sqb_destroy(sqb_ctx *ctx);
+int sqb_set_precision(sqb_ctx *ctx, int precision);
+int sqb_set_allreduce(sqb_ctx *ctx, sqb_allreduce_fn fn, void *user);
+/* Nodes processed per persistent CTA batch and CTAs per SM (0 = automatic). */
+int sqb_set_launch(sqb_ctx *ctx, int ctas_per_sm, int cols_per_thread);
+
+/* Veff on the block with its Rcut halo: the state of DS_SQ::Veff after the
+ * halo exchange of sq.cpp:400-492. */
+int sqb_set_veff(sqb_ctx *ctx, const double *veff_ext);
+
+/* Atom types and the replica atoms whose rc-ball meets the block + Rcut
+ * region (Replica_atoms_Rcut, initialize.cpp:1003-1196), type-major as
+ * DS_Atm::R{x,y,z}[a].ProcAtmRcut[r] lists them.  rep_atom is the global
+ * type-major atom index the force is accumulated into. */
+int sqb_set_atoms(sqb_ctx *ctx, int n_typ, const sqb_species *types, int n_rep, const int *rep_type,
+                  const int *rep_atom, const double *rep_xyz, int n_atm);
+
+/* NonlocalProjectors (nonlocal.cpp:317-518): UdVtm on every replica's ball,
+ * computed on the device from the radial tables.  If udvtm_out is not NULL
+ * the tables are also copied out, concatenated in replica order, each
+ * [nproj][(2nlocc+1)^3] as DS_ProcAtmRcut::UdVtm holds them. */
+int sqb_nonlocal_projectors(sqb_ctx *ctx, double *udvtm_out);
+/* Upload projector tables computed elsewhere (same layout as above). */
+int sqb_set_projectors(sqb_ctx *ctx, const double *udvtm);
+
+/* HsubTimesVec (sq.cpp:838-929) for `count` block nodes: vin and vout are
+ * [count][(2nloc+1)^3] window vectors. */
+int sqb_hsub_times_vec(sqb_ctx *ctx, int count, const int *nodes, const double *vin, double *vout);
+
+/* Lanczos bounds (LanczosAlgorithm, sq.cpp:965-1092) and Chebyshev moments
+ * (sq.cpp:530-661) of every block node.  Any output pointer may be NULL. */
+int sqb_lanczos_moments(sqb_ctx *ctx, double *chi, double *zee, double *rho_pj, int *lanczos_iters,
+                        double *lambda_min, double *lambda_max);
+
+/* NeConstraint (sq.cpp:1183-1228) on the moments of the last
+ * sqb_lanczos_moments call: 2 h^3 sum rho_pj.c(lambda) - N_e, reduced over
+ * ranks through the allreduce hook. */
+int sqb_ne_constraint(sqb_ctx *ctx, double lambda_f, double *fval);
+
+/* Fermi level as sq.cpp:669-731 finds it: BrentsAlgorithm (sq.cpp:1289) or
+ * NewtonRaphson (sq.cpp:1459) by grid->fermi_alg.  For scf_iter <= 1 the
+ * bracket is the global Lanczos range +-1, else lambda_warm +-2. */
+int sqb_fermi_level(sqb_ctx *ctx, int scf_iter, double lambda_warm, double *lambda_f, int *iters);
+
+/* Density, Fermi coefficients, band and entropy energies (sq.cpp:733-797). */
+int sqb_density_energy(sqb_ctx *ctx, double lambda_f, double *rho, double *ci, double *ebs, double *eent);
+
+/* ClenshawCurtisSpectralQuadrature (sq.cpp:377-834) end to end: the three
+ * calls above.  lambda_f is the warm start in and the Fermi level out. */
+int sqb_spectral_quadrature(sqb_ctx *ctx, int scf_iter, double *lambda_f, double *rho, double *rho_pj, double *ci,
+                            double *chi, double *zee, double *ebs, double *eent);
+
+/* ForcesNonLocal (forces.cpp:318-578) with chi, zee, Ci of the last
+ * sqb_spectral_quadrature call (or given ones when not NULL). */
+int sqb_forces_nonlocal(sqb_ctx *ctx, const double *chi, const double *zee, const double *ci, double *forces);
+
+int sqb_get_stats(const sqb_ctx *ctx, sqb_stats *out);
+const char *sqb_status_string(int status);
+/* Library version string. */
+const char *sqb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -153,7 +153,12 @@ class Case:
 
 def load_case(path) -> Case:
     """Read a case container written by the reference driver or the exporter."""
-    a = read_container(path)
+    return case_from_arrays(read_container(path))
+
+
+def case_from_arrays(a: dict) -> Case:
+    """Build a Case from container arrays; the radial tables ``psd<t>`` may be
+    absent (then only supplied projector tables can be used)."""
     pi = a["params_i"]
     pd = a["params_d"]
     n_typ = int(pi[13])
@@ -163,7 +168,7 @@ def load_case(path) -> Case:
         td = a["typ_d"][t]
         types.append(AtomType(natm=int(ti[0]), lmax=int(ti[1]), lloc=int(ti[2]), nlocc=int(ti[3]),
                               nproj=int(ti[5]), rc=float(td[0]), denom=td[1:5].copy(), z=float(td[5]),
-                              tables=a[f"psd{t}"]))
+                              tables=a.get(f"psd{t}", np.zeros((19, 0)))))
     return Case(
         n_int=tuple(int(x) for x in pi[0:3]), np_=tuple(int(x) for x in pi[3:6]),
         pnode_s=tuple(int(x) for x in pi[6:9]), nloc=int(pi[9]), fdn=int(pi[10]), npl=int(pi[11]),

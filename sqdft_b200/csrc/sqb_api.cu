@@ -1,0 +1,828 @@
+// C-ABI of sqdft_b200 (include/sqdft_b200.h): context management, uploads and
+// the host-side control flow of the SQ step.
+//
+// The device does the per-node work (node kernel), the per-node Chebyshev
+// coefficients and their reductions; the host keeps the reference's scalar
+// control flow -- Brent / Newton for the Fermi level and the order of the
+// phases of ClenshawCurtisSpectralQuadrature (sq.cpp:377-834) -- so the
+// sequence of trial Fermi levels is the reference's.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/sqdft_b200.h"
+#include "sqb_internal.cuh"
+
+using namespace sqb;
+
+struct sqb_ctx {
+  sqb_grid g{};
+  int device = 0, sms = 148;
+  cudaStream_t stream = nullptr;
+  int precision = SQB_FP64;
+  int cols = 0, ctas_per_sm = 1;
+  int n = 0, nnode = 0, ex = 0, ey = 0, ez = 0;
+  double h3 = 0.0;
+  sqb_allreduce_fn allreduce = nullptr;
+  void *allreduce_user = nullptr;
+
+  double *d_veff64 = nullptr;
+  float *d_veff32 = nullptr;
+  bool have_veff = false;
+
+  int n_typ = 0, n_rep = 0, n_atm = 0;
+  std::vector<int> typ_nproj, typ_nlocc;
+  int *d_rep_nn = nullptr, *d_rep_atom = nullptr;
+  long long *d_rep_off = nullptr, *d_typ_tab = nullptr;
+  int *d_typ_nlocc = nullptr, *d_typ_nproj = nullptr, *d_typ_lmax = nullptr, *d_typ_lloc = nullptr;
+  int *d_typ_size = nullptr;
+  double *d_proj_denom = nullptr, *d_tables = nullptr, *d_rep_xyz = nullptr;
+  bool have_tables = false;
+  double *d_tab64 = nullptr;
+  float *d_tab32 = nullptr;
+  long long tab_total = 0;
+  bool have_atoms = false, have_proj = false;
+
+  unsigned char *d_scratch = nullptr;
+  size_t scratch_stride = 0, scratch_bytes = 0;
+  int *d_counter = nullptr, *d_nodes = nullptr, *d_status = nullptr, *d_iters = nullptr;
+  unsigned long long *d_proj_points = nullptr;
+  double *d_chi = nullptr, *d_zee = nullptr, *d_rho_pj = nullptr, *d_lmin = nullptr, *d_lmax = nullptr;
+  bool have_moments = false;
+  double lmin_all = 0.0, lmax_all = 0.0;
+
+  double *d_xk = nullptr, *d_ctab = nullptr, *d_partial = nullptr, *d_result = nullptr;
+  double *d_rho = nullptr, *d_ci = nullptr;
+  bool have_ci = false;
+  double *d_fslots = nullptr, *d_f = nullptr;
+  double *d_tmp = nullptr;
+  size_t tmp_bytes = 0;
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  sqb_stats stats{};
+};
+
+namespace {
+
+#define CK(x)                                    \
+  do {                                           \
+    cudaError_t e_ = (x);                        \
+    if (e_ != cudaSuccess) {                     \
+      std::fprintf(stderr, "sqdft_b200: %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return SQB_ERR_CUDA;                       \
+    }                                            \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  return cudaMalloc((void **)p, count * sizeof(T) + 16);
+}
+
+// Nearest grid node of an atom coordinate with the midpoint rule of
+// nonlocal.cpp:49-64 (Replica_atoms_Rcut uses the same rule).
+int nearest_node(double c, double h) {
+  int n = (int)round(c / h);
+  if (fabs(fabs(n * h - c) - h * 0.5) < 1e-12) n = (int)floor((c / h) - 10 * 1e-12);
+  return n;
+}
+
+int reduce(sqb_ctx *c, double *v, int count, int op) {
+  if (!c->allreduce) return SQB_OK;
+  return c->allreduce(v, count, op, c->allreduce_user) == 0 ? SQB_OK : SQB_ERR_ARG;
+}
+
+int status_to_err(int st) {
+  if (st & ST_CAPACITY) return SQB_ERR_CAPACITY;
+  if (st & ST_FSLOTS) return SQB_ERR_CAPACITY;
+  if (st & ST_SPLINE_RANGE) return SQB_ERR_SPLINE_RANGE;
+  if (st & ST_NONFINITE) return SQB_ERR_NONFINITE;
+  if (st & ST_LANCZOS_MAXITER) return SQB_ERR_LANCZOS_MAXITER;
+  return SQB_OK;
+}
+
+int ensure_tmp(sqb_ctx *c, size_t bytes) {
+  if (c->tmp_bytes >= bytes) return SQB_OK;
+  if (c->d_tmp) cudaFree(c->d_tmp);
+  c->d_tmp = nullptr;
+  CK(cudaMalloc((void **)&c->d_tmp, bytes));
+  c->tmp_bytes = bytes;
+  return SQB_OK;
+}
+
+int choose_cols(const sqb_ctx *c) {
+  if (c->cols > 0) return c->cols;
+  return 2;
+}
+
+int ensure_scratch(sqb_ctx *c, int grid) {
+  const size_t nw = (size_t)c->n * c->n * c->n;
+  c->scratch_stride = ((4 * nw * sizeof(double)) + 255) & ~size_t(255);
+  const size_t need = c->scratch_stride * (size_t)grid;
+  if (c->scratch_bytes < need) {
+    if (c->d_scratch) cudaFree(c->d_scratch);
+    c->d_scratch = nullptr;
+    CK(cudaMalloc((void **)&c->d_scratch, need));
+    c->scratch_bytes = need;
+  }
+  return SQB_OK;
+}
+
+void fill_node_args(sqb_ctx *c, NodeArgs &a) {
+  std::memset(&a, 0, sizeof(a));
+  a.n = c->n;
+  a.nloc = c->g.nloc;
+  for (int d = 0; d < 3; d++) {
+    a.np[d] = c->g.np[d];
+    a.pnode_s[d] = c->g.pnode_s[d];
+  }
+  a.ex = c->ex;
+  a.ey = c->ey;
+  a.npl = c->g.npl;
+  a.h3 = c->h3;
+  a.lanczos_tol = c->g.lanczos_tol;
+  for (int k = 0; k <= FDN; k++) {
+    a.coeff_lap[k] = c->g.coeff_lap[k];
+    a.coeff_grad[k] = c->g.coeff_grad[k];
+  }
+  a.veff64 = c->d_veff64;
+  a.veff32 = c->d_veff32;
+  a.at.n_rep = c->n_rep;
+  a.at.rep_nn = c->d_rep_nn;
+  a.at.rep_atom = c->d_rep_atom;
+  a.at.rep_off = c->d_rep_off;
+  a.at.typ_nlocc = c->d_typ_nlocc;
+  a.at.typ_nproj = c->d_typ_nproj;
+  a.at.proj_denom = c->d_proj_denom;
+  a.at.tab64 = c->d_tab64;
+  a.at.tab32 = c->d_tab32;
+  a.counter = c->d_counter;
+  a.status = c->d_status;
+  a.mixed = c->precision == SQB_FP32_MIXED;
+  a.proj_points = c->d_proj_points;
+}
+
+// Launch the node kernel over `count` nodes of d_list; returns SQB status.
+int run_nodes(sqb_ctx *c, NodeArgs &a, const int *d_list, int count) {
+  const int cols = choose_cols(c);
+  const int threads = node_kernel_threads(c->n, cols);
+  if (threads > 1024) return SQB_ERR_UNSUPPORTED;
+  int grid = c->sms * (c->ctas_per_sm > 0 ? c->ctas_per_sm : 1);
+  if (grid > count) grid = count;
+  if (grid < 1) grid = 1;
+  int rc = ensure_scratch(c, grid);
+  if (rc) return rc;
+  a.scratch = c->d_scratch;
+  a.scratch_stride = c->scratch_stride;
+  a.node_list = d_list;
+  a.n_list = count;
+  CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->d_proj_points, 0, sizeof(unsigned long long), c->stream));
+  CK(launch_node_kernel(a, grid, cols, c->stream));
+  return SQB_OK;
+}
+
+int read_status(sqb_ctx *c) {
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return status_to_err(st);
+}
+
+FermiArgs fermi_args(sqb_ctx *c) {
+  FermiArgs f{};
+  f.n_nodes = c->nnode;
+  f.npl = c->g.npl;
+  f.bet0 = c->g.bet;
+  f.h3 = c->h3;
+  f.chi = c->d_chi;
+  f.zee = c->d_zee;
+  f.rho_pj = c->d_rho_pj;
+  f.xk = c->d_xk;
+  f.ctab = c->d_ctab;
+  f.partial = c->d_partial;
+  f.result = c->d_result;
+  f.rho = c->d_rho;
+  f.ci = c->d_ci;
+  f.status = c->d_status;
+  return f;
+}
+
+// NeConstraint / NeConstraint_derv: g (and dg) before the h^3 scaling,
+// summed over ranks.
+int ne_sums(sqb_ctx *c, double lambda, int deriv, double *g, double *dg) {
+  CK(launch_ne_constraint(fermi_args(c), lambda, deriv, c->stream));
+  double r[2];
+  CK(cudaMemcpyAsync(r, c->d_result, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->stats.kernel_launches += 2;
+  *g = r[0];
+  *dg = r[1];
+  return SQB_OK;
+}
+
+int ne_constraint(sqb_ctx *c, double lambda, double *fval) {
+  double g, dg;
+  int rc = ne_sums(c, lambda, 0, &g, &dg);
+  if (rc) return rc;
+  g = g * pow(c->g.delta, 3);  // sq.cpp:1214
+  rc = reduce(c, &g, 1, SQB_SUM);
+  if (rc) return rc;
+  *fval = g - (-c->g.ncharge);
+  return std::isfinite(*fval) ? SQB_OK : SQB_ERR_NONFINITE;
+}
+
+#define SIGN(a, b) ((b) >= 0.0 ? fabs(a) : -fabs(a))
+
+// BrentsAlgorithm (sq.cpp:1289-1404), same control flow and tolerances.
+int brent(sqb_ctx *c, double x1, double x2, int scf_iter, double lambda_warm, double *root, int *iters) {
+  const double EPS = 2.5e-16, tol = c->g.fermi_tol;
+  double tol1q, eq, a = x1, b = x2, cc = x2, d = 0.0, e = 0.0, min1, min2;
+  if (scf_iter > 1) {
+    a = lambda_warm - 2;
+    b = lambda_warm + 2;
+  }
+  double fa, fb, fc, p, q, r, s, tol1, xm;
+  int rc = ne_constraint(c, a, &fa);
+  if (!rc) rc = ne_constraint(c, b, &fb);
+  if (rc) return rc;
+  if ((fa > 0.0 && fb > 0.0) || (fa < 0.0 && fb < 0)) return SQB_ERR_NOT_BRACKETED;
+  fc = fb;
+  for (int iter = 1; iter <= 100; iter++) {
+    if ((fb > 0.0 && fc > 0.0) || (fb < 0.0 && fc < 0.0)) {
+      cc = a;
+      fc = fa;
+      e = d = b - a;
+    }
+    if (fabs(fc) < fabs(fb)) {
+      a = b;
+      b = cc;
+      cc = a;
+      fa = fb;
+      fb = fc;
+      fc = fa;
+    }
+    tol1 = 2.0 * EPS * fabs(b) + 0.5 * tol;
+    xm = 0.5 * (cc - b);
+    if (fabs(xm) <= tol1 || fb == 0.0) {
+      *root = b;
+      *iters = iter;
+      return SQB_OK;
+    }
+    if (fabs(e) >= tol1 && fabs(fa) > fabs(fb)) {
+      s = fb / fa;
+      if (a == cc) {
+        p = 2.0 * xm * s;
+        q = 1.0 - s;
+      } else {
+        q = fa / fc;
+        r = fb / fc;
+        p = s * (2.0 * xm * q * (q - r) - (b - a) * (r - 1.0));
+        q = (q - 1.0) * (r - 1.0) * (s - 1.0);
+      }
+      if (p > 0.0) q = -q;
+      p = fabs(p);
+      tol1q = tol1 * q;
+      min1 = 3.0 * xm * q - fabs(tol1q);
+      eq = e * q;
+      min2 = fabs(eq);
+      if (2.0 * p < (min1 < min2 ? min1 : min2)) {
+        e = d;
+        d = p / q;
+      } else {
+        d = xm;
+        e = d;
+      }
+    } else {
+      d = xm;
+      e = d;
+    }
+    a = b;
+    fa = fb;
+    if (fabs(d) > tol1) b += d;
+    else b += SIGN(tol1, xm);
+    rc = ne_constraint(c, b, &fb);
+    if (rc) return rc;
+  }
+  return SQB_ERR_FERMI_MAXITER;
+}
+
+// NewtonRaphson (sq.cpp:1459-1490) with NeConstraint_derv (sq.cpp:1407-1449).
+int newton(sqb_ctx *c, double lambda0, double *root, int *iters) {
+  double lnew = 0.0, lold = lambda0, err = 1.0;
+  int count = 0;
+  while (err > c->g.fermi_tol && count < 200) {
+    double g, dg;
+    int rc = ne_sums(c, lold, 1, &g, &dg);
+    if (rc) return rc;
+    dg = dg * c->g.bet;
+    dg = dg * pow(c->g.delta, 3);
+    g = g * pow(c->g.delta, 3);
+    double t[2] = {g, dg};
+    rc = reduce(c, t, 2, SQB_SUM);
+    if (rc) return rc;
+    const double fa = t[0] - (-c->g.ncharge), dfa = t[1];
+    lnew = lold - (fa / dfa);
+    err = fabs(lnew - lold);
+    lold = lnew;
+    count += 1;
+  }
+  *root = lnew;
+  *iters = count;
+  return std::isfinite(lnew) ? SQB_OK : SQB_ERR_NONFINITE;
+}
+
+float elapsed(sqb_ctx *c) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  return ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *sqb_version(void) { return "sqdft_b200 0.1 (sm_100a)"; }
+
+const char *sqb_status_string(int st) {
+  switch (st) {
+    case SQB_OK: return "ok";
+    case SQB_ERR_ARG: return "invalid argument";
+    case SQB_ERR_CUDA: return "CUDA error";
+    case SQB_ERR_UNSUPPORTED: return "unsupported configuration";
+    case SQB_ERR_NOT_BRACKETED: return "Root must be bracketed in Brent's method";
+    case SQB_ERR_FERMI_MAXITER: return "Maximum iterations exceeded in brents root finding method";
+    case SQB_ERR_NEGATIVE_RHO: return "Element of rho is negative";
+    case SQB_ERR_LANCZOS_MAXITER: return "Lanczos exceeded max_iter";
+    case SQB_ERR_DENOM_ZERO: return "Denom=0.0 in Nonlocal";
+    case SQB_ERR_SPLINE_RANGE: return "out of range in spline interpolation";
+    case SQB_ERR_CAPACITY: return "too many projector atoms in one truncation window";
+    case SQB_ERR_NONFINITE: return "non-finite value";
+    case SQB_ERR_STATE: return "inputs not set";
+    default: return "unknown status";
+  }
+}
+
+int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out) {
+  if (!grid || !out) return SQB_ERR_ARG;
+  *out = nullptr;
+  const sqb_grid &g = *grid;
+  for (int d = 0; d < 3; d++)
+    if (g.np[d] <= 0 || g.n_int[d] <= 0) return SQB_ERR_ARG;
+  if (g.nloc < 1 || g.npl < 4 || g.npl % 4 != 0 || !(g.delta > 0) || !(g.bet > 0)) return SQB_ERR_ARG;
+  if (g.fdn != FDN) return SQB_ERR_UNSUPPORTED;
+  if (g.fermi_alg != 1 && g.fermi_alg != 2) return SQB_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) return SQB_ERR_CUDA;
+  sqb_ctx *c = new sqb_ctx();
+  c->g = g;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete c;
+    return SQB_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  c->n = 2 * g.nloc + 1;
+  if (node_kernel_threads(c->n, 2) > 1024) {
+    delete c;
+    return SQB_ERR_UNSUPPORTED;
+  }
+  c->nnode = g.np[0] * g.np[1] * g.np[2];
+  c->ex = g.np[0] + 2 * g.nloc;
+  c->ey = g.np[1] + 2 * g.nloc;
+  c->ez = g.np[2] + 2 * g.nloc;
+  c->h3 = pow(g.delta, 3);
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&c->ev0));
+  CK(cudaEventCreate(&c->ev1));
+  CK(node_kernel_setup(c->n));
+  const size_t N = c->nnode, K = g.npl + 1;
+  CK(dalloc(&c->d_counter, 1));
+  CK(dalloc(&c->d_status, 1));
+  CK(dalloc(&c->d_proj_points, 1));
+  CK(dalloc(&c->d_nodes, N));
+  CK(dalloc(&c->d_iters, N));
+  CK(dalloc(&c->d_chi, N));
+  CK(dalloc(&c->d_zee, N));
+  CK(dalloc(&c->d_lmin, N));
+  CK(dalloc(&c->d_lmax, N));
+  CK(dalloc(&c->d_rho, N));
+  CK(dalloc(&c->d_rho_pj, N * K));
+  CK(dalloc(&c->d_ci, N * K));
+  CK(dalloc(&c->d_xk, K));
+  CK(dalloc(&c->d_ctab, K * K));
+  CK(dalloc(&c->d_partial, (size_t)2 * (c->sms + 8)));
+  CK(dalloc(&c->d_result, 4));
+  std::vector<int> nodes(N);
+  for (size_t i = 0; i < N; i++) nodes[i] = (int)i;
+  CK(cudaMemcpy(c->d_nodes, nodes.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+  // Chebyshev-Gauss nodes and cosine table with the expressions of
+  // sq.cpp:1239-1255, so the values are the reference's.
+  const int npl = g.npl;
+  std::vector<double> xk(K), ctab(K * K);
+  for (int k = 0; k < npl + 1; k++) xk[k] = cos(M_PI * ((double)((k - 0.5 + 1) / (npl + 1))));
+  for (int j = 0; j < npl + 1; j++)
+    for (int k = 0; k < npl + 1; k++) ctab[(size_t)j * K + k] = cos((M_PI * (j - 1 + 1)) * ((double)((k - 0.5 + 1) / (npl + 1))));
+  CK(cudaMemcpy(c->d_xk, xk.data(), K * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_ctab, ctab.data(), K * K * sizeof(double), cudaMemcpyHostToDevice));
+  c->stats.window_points = (long long)c->n * c->n * c->n;
+  *out = c;
+  return SQB_OK;
+}
+
+int sqb_destroy(sqb_ctx *c) {
+  if (!c) return SQB_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  void *ptrs[] = {c->d_veff64, c->d_veff32, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
+                  c->d_typ_nlocc, c->d_typ_nproj, c->d_typ_lmax, c->d_typ_lloc, c->d_typ_size, c->d_proj_denom,
+                  c->d_tables, c->d_rep_xyz, c->d_tab64, c->d_tab32, c->d_scratch, c->d_counter, c->d_nodes,
+                  c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
+                  c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
+                  c->d_f, c->d_tmp};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return SQB_OK;
+}
+
+int sqb_set_precision(sqb_ctx *c, int precision) {
+  if (!c || (precision != SQB_FP64 && precision != SQB_FP32_MIXED)) return SQB_ERR_ARG;
+  c->precision = precision;
+  return SQB_OK;
+}
+
+int sqb_set_allreduce(sqb_ctx *c, sqb_allreduce_fn fn, void *user) {
+  if (!c) return SQB_ERR_ARG;
+  c->allreduce = fn;
+  c->allreduce_user = user;
+  return SQB_OK;
+}
+
+int sqb_set_launch(sqb_ctx *c, int ctas_per_sm, int cols_per_thread) {
+  if (!c || ctas_per_sm < 0 || ctas_per_sm > 4 || cols_per_thread < 0 || cols_per_thread > 2) return SQB_ERR_ARG;
+  if (cols_per_thread > 0 && node_kernel_threads(c->n, cols_per_thread) > 1024) return SQB_ERR_UNSUPPORTED;
+  c->ctas_per_sm = ctas_per_sm > 0 ? ctas_per_sm : 1;
+  c->cols = cols_per_thread;
+  return SQB_OK;
+}
+
+int sqb_set_veff(sqb_ctx *c, const double *veff_ext) {
+  if (!c || !veff_ext) return SQB_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)c->ex * c->ey * c->ez;
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(veff_ext[i])) return SQB_ERR_NONFINITE;
+  if (!c->d_veff64) {
+    CK(dalloc(&c->d_veff64, n));
+    CK(dalloc(&c->d_veff32, n));
+  }
+  CK(cudaMemcpyAsync(c->d_veff64, veff_ext, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_to_float(c->d_veff64, c->d_veff32, (long long)n, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_veff = true;
+  c->have_moments = false;
+  return SQB_OK;
+}
+
+int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, const int *rep_type,
+                  const int *rep_atom, const double *rep_xyz, int n_atm) {
+  if (!c || n_typ < 0 || n_rep < 0 || n_atm < 0 || (n_typ > 0 && !types)) return SQB_ERR_ARG;
+  if (n_rep > 0 && (!rep_type || !rep_atom || !rep_xyz)) return SQB_ERR_ARG;
+  cudaSetDevice(c->device);
+  c->n_typ = n_typ;
+  c->n_rep = n_rep;
+  c->n_atm = n_atm;
+  c->typ_nproj.assign(n_typ, 0);
+  c->typ_nlocc.assign(n_typ, 0);
+  std::vector<int> lmax(n_typ), lloc(n_typ), size(n_typ);
+  std::vector<long long> ttab(n_typ);
+  std::vector<double> denom((size_t)std::max(n_typ, 1) * MAXPROJ_TYPE, 0.0);
+  long long tables_len = 0;
+  bool all_tables = n_typ > 0;
+  for (int t = 0; t < n_typ; t++) {
+    const sqb_species &s = types[t];
+    if (s.lmax < 0 || s.lmax > 3 || s.nlocc < 0 || s.natm < 0) return SQB_ERR_ARG;
+    int np = 0;
+    for (int l = 0; l <= s.lmax; l++) {
+      if (l == s.lloc) continue;
+      for (int m = -l; m <= l; m++) denom[(size_t)t * MAXPROJ_TYPE + np++] = s.denom[l];
+      if (s.denom[l] == 0.0) return SQB_ERR_DENOM_ZERO;  // nonlocal.cpp:163
+    }
+    c->typ_nproj[t] = np;
+    c->typ_nlocc[t] = s.nlocc;
+    lmax[t] = s.lmax;
+    lloc[t] = s.lloc;
+    size[t] = s.size;
+    ttab[t] = tables_len;
+    if (s.tables && s.size >= 3) tables_len += 19LL * s.size;
+    else all_tables = false;
+  }
+  std::vector<int> nn((size_t)4 * std::max(n_rep, 1));
+  std::vector<long long> off(std::max(n_rep, 1));
+  long long total = 0;
+  for (int r = 0; r < n_rep; r++) {
+    const int t = rep_type[r];
+    if (t < 0 || t >= n_typ || rep_atom[r] < 0 || rep_atom[r] >= n_atm) return SQB_ERR_ARG;
+    nn[4 * r] = nearest_node(rep_xyz[3 * r], c->g.delta);
+    nn[4 * r + 1] = nearest_node(rep_xyz[3 * r + 1], c->g.delta);
+    nn[4 * r + 2] = nearest_node(rep_xyz[3 * r + 2], c->g.delta);
+    nn[4 * r + 3] = t;
+    off[r] = total;
+    const long long S = 2LL * c->typ_nlocc[t] + 1;
+    total += c->typ_nproj[t] * S * S * S;
+  }
+  c->tab_total = total;
+  CK(dalloc(&c->d_rep_nn, nn.size()));
+  CK(dalloc(&c->d_rep_atom, std::max(n_rep, 1)));
+  CK(dalloc(&c->d_rep_off, off.size()));
+  CK(dalloc(&c->d_rep_xyz, (size_t)3 * std::max(n_rep, 1)));
+  CK(dalloc(&c->d_typ_nlocc, std::max(n_typ, 1)));
+  CK(dalloc(&c->d_typ_nproj, std::max(n_typ, 1)));
+  CK(dalloc(&c->d_typ_lmax, std::max(n_typ, 1)));
+  CK(dalloc(&c->d_typ_lloc, std::max(n_typ, 1)));
+  CK(dalloc(&c->d_typ_size, std::max(n_typ, 1)));
+  CK(dalloc(&c->d_typ_tab, std::max(n_typ, 1)));
+  CK(dalloc(&c->d_proj_denom, denom.size()));
+  CK(dalloc(&c->d_tab64, (size_t)std::max(total, 1LL)));
+  CK(dalloc(&c->d_tab32, (size_t)std::max(total, 1LL)));
+  CK(dalloc(&c->d_fslots, (size_t)c->nnode * FSLOTS * 4));
+  CK(dalloc(&c->d_f, (size_t)3 * std::max(n_atm, 1)));
+  CK(cudaMemcpy(c->d_rep_nn, nn.data(), nn.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (n_rep > 0) {
+    CK(cudaMemcpy(c->d_rep_atom, rep_atom, n_rep * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_rep_xyz, rep_xyz, (size_t)3 * n_rep * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(c->d_rep_off, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  if (n_typ > 0) {
+    CK(cudaMemcpy(c->d_typ_nlocc, c->typ_nlocc.data(), n_typ * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_typ_nproj, c->typ_nproj.data(), n_typ * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_typ_lmax, lmax.data(), n_typ * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_typ_lloc, lloc.data(), n_typ * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_typ_size, size.data(), n_typ * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_typ_tab, ttab.data(), n_typ * sizeof(long long), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(c->d_proj_denom, denom.data(), denom.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c->have_tables = all_tables;
+  if (all_tables) {
+    CK(dalloc(&c->d_tables, (size_t)tables_len));
+    for (int t = 0; t < n_typ; t++)
+      CK(cudaMemcpy(c->d_tables + ttab[t], types[t].tables, 19ULL * types[t].size * sizeof(double),
+                    cudaMemcpyHostToDevice));
+  }
+  c->have_atoms = true;
+  c->have_proj = total == 0;
+  c->have_moments = false;
+  return SQB_OK;
+}
+
+int sqb_nonlocal_projectors(sqb_ctx *c, double *udvtm_out) {
+  if (!c) return SQB_ERR_ARG;
+  if (!c->have_atoms || !c->have_tables) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  ProjArgs p{};
+  p.n_rep = c->n_rep;
+  p.delta = c->g.delta;
+  p.rep_nn = c->d_rep_nn;
+  p.rep_xyz = c->d_rep_xyz;
+  p.rep_off = c->d_rep_off;
+  p.typ_nlocc = c->d_typ_nlocc;
+  p.typ_lmax = c->d_typ_lmax;
+  p.typ_lloc = c->d_typ_lloc;
+  p.typ_size = c->d_typ_size;
+  p.typ_tab = c->d_typ_tab;
+  p.tables = c->d_tables;
+  p.out64 = c->d_tab64;
+  p.out32 = c->d_tab32;
+  p.total = c->tab_total;
+  p.status = c->d_status;
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  CK(cudaEventRecord(c->ev0, c->stream));
+  CK(launch_projectors(p, c->stream));
+  CK(cudaEventRecord(c->ev1, c->stream));
+  int rc = read_status(c);
+  c->stats.ms_projectors = elapsed(c);
+  if (rc) return rc;
+  if (udvtm_out && c->tab_total > 0)
+    CK(cudaMemcpy(udvtm_out, c->d_tab64, (size_t)c->tab_total * sizeof(double), cudaMemcpyDeviceToHost));
+  c->have_proj = true;
+  c->have_moments = false;
+  return SQB_OK;
+}
+
+int sqb_set_projectors(sqb_ctx *c, const double *udvtm) {
+  if (!c || (!udvtm && c->tab_total > 0)) return SQB_ERR_ARG;
+  if (!c->have_atoms) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  if (c->tab_total > 0) {
+    CK(cudaMemcpyAsync(c->d_tab64, udvtm, (size_t)c->tab_total * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(launch_to_float(c->d_tab64, c->d_tab32, c->tab_total, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  c->have_proj = true;
+  c->have_moments = false;
+  return SQB_OK;
+}
+
+int sqb_hsub_times_vec(sqb_ctx *c, int count, const int *nodes, const double *vin, double *vout) {
+  if (!c || count < 0 || (count > 0 && (!nodes || !vin || !vout))) return SQB_ERR_ARG;
+  if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
+  if (count == 0) return SQB_OK;
+  for (int i = 0; i < count; i++)
+    if (nodes[i] < 0 || nodes[i] >= c->nnode) return SQB_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t nw = (size_t)c->n * c->n * c->n;
+  int rc = ensure_tmp(c, (2 * nw * count) * sizeof(double) + count * sizeof(int) + 64);
+  if (rc) return rc;
+  double *d_in = c->d_tmp, *d_out = c->d_tmp + nw * count;
+  int *d_list = reinterpret_cast<int *>(d_out + nw * count);
+  CK(cudaMemcpyAsync(d_in, vin, nw * count * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(d_list, nodes, count * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  NodeArgs a;
+  fill_node_args(c, a);
+  a.mode = MODE_APPLY;
+  a.apply_in = d_in;
+  a.apply_out = d_out;
+  rc = run_nodes(c, a, d_list, count);
+  if (rc) return rc;
+  rc = read_status(c);
+  if (rc) return rc;
+  CK(cudaMemcpy(vout, d_out, nw * count * sizeof(double), cudaMemcpyDeviceToHost));
+  return SQB_OK;
+}
+
+int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, int *lanczos_iters,
+                        double *lambda_min, double *lambda_max) {
+  if (!c) return SQB_ERR_ARG;
+  if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  NodeArgs a;
+  fill_node_args(c, a);
+  a.mode = MODE_SQ;
+  a.chi = c->d_chi;
+  a.zee = c->d_zee;
+  a.rho_pj = c->d_rho_pj;
+  a.lmin = c->d_lmin;
+  a.lmax = c->d_lmax;
+  a.lanczos_iters = c->d_iters;
+  c->stats.kernel_launches = 0;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = run_nodes(c, a, c->d_nodes, c->nnode);
+  if (rc) return rc;
+  CK(launch_minmax(c->d_lmin, c->d_lmax, c->nnode, c->d_result, c->stream));
+  CK(cudaEventRecord(c->ev1, c->stream));
+  c->stats.kernel_launches += 2;
+  rc = read_status(c);
+  c->stats.ms_lanczos_moments = elapsed(c);
+  if (rc) return rc;
+  double mm[2];
+  CK(cudaMemcpy(mm, c->d_result, sizeof(mm), cudaMemcpyDeviceToHost));
+  rc = reduce(c, &mm[0], 1, SQB_MIN);
+  if (!rc) rc = reduce(c, &mm[1], 1, SQB_MAX);
+  if (rc) return rc;
+  c->lmin_all = mm[0];
+  c->lmax_all = mm[1];
+  const size_t N = c->nnode, K = c->g.npl + 1;
+  std::vector<int> its(N);
+  CK(cudaMemcpy(its.data(), c->d_iters, N * sizeof(int), cudaMemcpyDeviceToHost));
+  unsigned long long pp = 0;
+  CK(cudaMemcpy(&pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
+  long long sum = 0;
+  int mx = 0;
+  for (size_t i = 0; i < N; i++) {
+    sum += its[i];
+    mx = std::max(mx, its[i]);
+  }
+  c->stats.lanczos_iters = sum;
+  c->stats.max_lanczos_iters = mx;
+  // passes: Lanczos 2 per iteration + 2, Chebyshev npl/2 (matvec passes only)
+  c->stats.matvecs = (sum + 1) + (long long)N * (c->g.npl / 2);
+  c->stats.proj_points = (long long)pp;
+  if (lanczos_iters) std::memcpy(lanczos_iters, its.data(), N * sizeof(int));
+  if (chi) CK(cudaMemcpy(chi, c->d_chi, N * sizeof(double), cudaMemcpyDeviceToHost));
+  if (zee) CK(cudaMemcpy(zee, c->d_zee, N * sizeof(double), cudaMemcpyDeviceToHost));
+  if (rho_pj) CK(cudaMemcpy(rho_pj, c->d_rho_pj, N * K * sizeof(double), cudaMemcpyDeviceToHost));
+  if (lambda_min) CK(cudaMemcpy(lambda_min, c->d_lmin, N * sizeof(double), cudaMemcpyDeviceToHost));
+  if (lambda_max) CK(cudaMemcpy(lambda_max, c->d_lmax, N * sizeof(double), cudaMemcpyDeviceToHost));
+  c->have_moments = true;
+  c->have_ci = false;
+  return SQB_OK;
+}
+
+int sqb_ne_constraint(sqb_ctx *c, double lambda_f, double *fval) {
+  if (!c || !fval) return SQB_ERR_ARG;
+  if (!c->have_moments) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  return ne_constraint(c, lambda_f, fval);
+}
+
+int sqb_fermi_level(sqb_ctx *c, int scf_iter, double lambda_warm, double *lambda_f, int *iters) {
+  if (!c || !lambda_f) return SQB_ERR_ARG;
+  if (!c->have_moments) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  int it = 0, rc;
+  double root = 0.0;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  if (c->g.fermi_alg == 1) rc = brent(c, c->lmin_all - 1, c->lmax_all + 1, scf_iter, lambda_warm, &root, &it);
+  else rc = newton(c, scf_iter <= 1 ? 0.2 : lambda_warm, &root, &it);  // sq.cpp:721-730
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  c->stats.ms_fermi = elapsed(c);
+  c->stats.fermi_iters = it;
+  if (rc) return rc;
+  *lambda_f = root;
+  if (iters) *iters = it;
+  return SQB_OK;
+}
+
+int sqb_density_energy(sqb_ctx *c, double lambda_f, double *rho, double *ci, double *ebs, double *eent) {
+  if (!c) return SQB_ERR_ARG;
+  if (!c->have_moments) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  CK(cudaEventRecord(c->ev0, c->stream));
+  CK(launch_density_energy(fermi_args(c), lambda_f, c->stream));
+  CK(cudaEventRecord(c->ev1, c->stream));
+  c->stats.kernel_launches += 2;
+  int st = 0;
+  double r[2];
+  CK(cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(r, c->d_result, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->stats.ms_density = elapsed(c);
+  c->have_ci = true;
+  if (st & 2) return SQB_ERR_NONFINITE;
+  int rc = reduce(c, r, 2, SQB_SUM);
+  if (rc) return rc;
+  const size_t N = c->nnode, K = c->g.npl + 1;
+  if (rho) CK(cudaMemcpy(rho, c->d_rho, N * sizeof(double), cudaMemcpyDeviceToHost));
+  if (ci) CK(cudaMemcpy(ci, c->d_ci, N * K * sizeof(double), cudaMemcpyDeviceToHost));
+  if (ebs) *ebs = r[0];
+  if (eent) *eent = r[1];
+  if (st & 1) return SQB_ERR_NEGATIVE_RHO;
+  return SQB_OK;
+}
+
+int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *rho, double *rho_pj, double *ci,
+                            double *chi, double *zee, double *ebs, double *eent) {
+  if (!c || !lambda_f) return SQB_ERR_ARG;
+  int rc = sqb_lanczos_moments(c, chi, zee, rho_pj, nullptr, nullptr, nullptr);
+  if (rc) return rc;
+  double lam = 0.0;
+  rc = sqb_fermi_level(c, scf_iter, *lambda_f, &lam, nullptr);
+  if (rc) return rc;
+  *lambda_f = lam;
+  return sqb_density_energy(c, lam, rho, ci, ebs, eent);
+}
+
+int sqb_forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const double *ci, double *forces) {
+  if (!c || !forces) return SQB_ERR_ARG;
+  if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  const size_t N = c->nnode, K = c->g.npl + 1;
+  if (chi || zee || ci) {
+    if (!chi || !zee || !ci) return SQB_ERR_ARG;
+    CK(cudaMemcpy(c->d_chi, chi, N * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_zee, zee, N * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_ci, ci, N * K * sizeof(double), cudaMemcpyHostToDevice));
+  } else if (!c->have_ci) {
+    return SQB_ERR_STATE;
+  }
+  NodeArgs a;
+  fill_node_args(c, a);
+  a.mode = MODE_FORCES;
+  a.chi_in = c->d_chi;
+  a.zee_in = c->d_zee;
+  a.ci = c->d_ci;
+  a.fslots = c->d_fslots;
+  c->stats.kernel_launches = 0;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = run_nodes(c, a, c->d_nodes, c->nnode);
+  if (rc) return rc;
+  CK(launch_force_reduce(c->d_fslots, c->nnode, c->n_atm, c->d_f, c->stream));
+  CK(cudaEventRecord(c->ev1, c->stream));
+  c->stats.kernel_launches += 2;
+  rc = read_status(c);
+  c->stats.ms_forces = elapsed(c);
+  if (rc) return rc;
+  if (c->n_atm > 0) CK(cudaMemcpy(forces, c->d_f, (size_t)3 * c->n_atm * sizeof(double), cudaMemcpyDeviceToHost));
+  return reduce(c, forces, 3 * c->n_atm, SQB_SUM);
+}
+
+int sqb_get_stats(const sqb_ctx *c, sqb_stats *out) {
+  if (!c || !out) return SQB_ERR_ARG;
+  *out = c->stats;
+  return SQB_OK;
+}
+
+}  // extern "C"

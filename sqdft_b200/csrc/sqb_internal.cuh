@@ -1,0 +1,116 @@
+// Internal declarations shared by the sqdft_b200 CUDA sources.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sqb {
+
+constexpr int FDN = 6;           // 12th-order stencil, the order the configurations use
+constexpr int MAXE = 128;        // projector-bearing replicas per node window
+constexpr int MAXP = 512;        // projector instances (replica x (l,m)) per node window
+constexpr int MAXL = 504;        // tridiagonal capacity: 500 Lanczos iterations + 2 (sq.cpp:967)
+constexpr int LANCZOS_MAX_ITER = 500;
+constexpr int MAXPROJ_TYPE = 16; // (l,m) pairs of one type, l <= 3
+constexpr int FSLOTS = 8;        // replicas whose ball holds one node (force contributions)
+
+// Device-side status bits (or-ed by the kernels, mapped to SQB_ERR_* on the host).
+enum : int {
+  ST_CAPACITY = 1,
+  ST_LANCZOS_MAXITER = 2,
+  ST_NONFINITE = 4,
+  ST_SPLINE_RANGE = 8,
+  ST_FSLOTS = 16,
+};
+
+// Replica atoms and projector tables as the node kernels read them.
+struct DevAtoms {
+  int n_rep;
+  const int *rep_nn;        // [n_rep][4]: nearest node x, y, z (global, reference tie rule), type
+  const int *rep_atom;      // [n_rep] global atom index
+  const long long *rep_off; // [n_rep] table offset (elements)
+  const int *typ_nlocc;     // [n_typ]
+  const int *typ_nproj;     // [n_typ]
+  const double *proj_denom; // [n_typ][MAXPROJ_TYPE]
+  const double *tab64;      // concatenated UdVtm, FP64
+  const float *tab32;       // the same in FP32 (mixed path)
+};
+
+enum NodeMode : int { MODE_SQ = 0, MODE_FORCES = 1, MODE_APPLY = 2 };
+
+struct NodeArgs {
+  int mode;
+  int mixed;     // 1: Chebyshev passes in FP32
+  int n;         // window edge 2*nloc+1
+  int nloc;
+  int np[3];
+  int pnode_s[3];
+  int ex, ey;    // Veff block + halo dims (x, y)
+  int npl;
+  double h3;     // pow(delta, 3)
+  double lanczos_tol;
+  double coeff_lap[FDN + 1];
+  double coeff_grad[FDN + 1];
+  const double *veff64;
+  const float *veff32;
+  DevAtoms at;
+  const int *node_list; // nodes to process
+  int n_list;
+  int *counter;         // work-queue head (zeroed before launch)
+  unsigned char *scratch;
+  size_t scratch_stride; // bytes per CTA
+  // MODE_SQ outputs, indexed by node id
+  double *chi, *zee, *rho_pj, *lmin, *lmax;
+  int *lanczos_iters;
+  // MODE_FORCES inputs / outputs
+  const double *chi_in, *zee_in, *ci;
+  double *fslots; // [n_list][FSLOTS][4]: atom, fx, fy, fz
+  // MODE_APPLY
+  const double *apply_in;
+  double *apply_out;
+  int *status;
+  unsigned long long *proj_points; // algorithmic projector-ball points touched
+};
+
+// Host-side launchers (sqb_node.cu).
+size_t node_kernel_smem(int n, int cols);
+int node_kernel_threads(int n, int cols);
+cudaError_t launch_node_kernel(const NodeArgs &a, int grid, int cols, cudaStream_t s);
+cudaError_t node_kernel_setup(int n);
+
+// Fermi-level and assembly kernels (sqb_fermi.cu).
+struct FermiArgs {
+  int n_nodes, npl;
+  double bet0, h3;
+  const double *chi, *zee, *rho_pj;
+  const double *xk;   // [npl+1] Chebyshev-Gauss nodes (sq.cpp:1241)
+  const double *ctab; // [npl+1][npl+1] cos(pi j (k+1/2)/(npl+1)) (sq.cpp:1250)
+  double *partial;    // per-block partial sums
+  double *result;     // final sums
+  double *rho, *ci;   // assembly outputs
+  int *status;
+};
+cudaError_t launch_ne_constraint(const FermiArgs &a, double lambda, int with_derivative, cudaStream_t s);
+cudaError_t launch_density_energy(const FermiArgs &a, double lambda, cudaStream_t s);
+int fermi_blocks(int n_nodes);
+
+// Force reduction and projector kernels.
+cudaError_t launch_force_reduce(const double *fslots, int n_list, int n_atm, double *f, cudaStream_t s);
+struct ProjArgs {
+  int n_rep;
+  double delta;
+  const int *rep_nn;
+  const double *rep_xyz;
+  const long long *rep_off;
+  const int *typ_nlocc, *typ_lmax, *typ_lloc, *typ_size;
+  const long long *typ_tab; // offset of each type's 19 x size tables
+  const double *tables;
+  double *out64;
+  float *out32;
+  long long total;
+  int *status;
+};
+cudaError_t launch_projectors(const ProjArgs &a, cudaStream_t s);
+cudaError_t launch_to_float(const double *in, float *out, long long n, cudaStream_t s);
+cudaError_t launch_minmax(const double *lmin, const double *lmax, int n, double *out, cudaStream_t s);
+
+}  // namespace sqb

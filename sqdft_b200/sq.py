@@ -1,0 +1,334 @@
+"""Python host mirror of SQDFT's SQ entry points over the sqdft_b200 C ABI.
+
+``SQState`` carries the DS_SQ fields the SQ step reads and writes
+(ds_sq.h:128-238) as numpy arrays; the functions ``NonlocalProjectors``,
+``ClenshawCurtisSpectralQuadrature`` and ``ForcesNonLocal`` fill the same
+fields as their reference namesakes (nonlocal.cpp:317, sq.cpp:377,
+forces.cpp:318).  All computation runs in the CUDA library
+(``sqdft_b200/_build/libsqdft_b200.so``); there is no CPU path, and a missing
+library is an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from .case import Case
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libsqdft_b200.so"
+
+SQB_FP64 = 0
+SQB_FP32_MIXED = 1
+SQB_SUM, SQB_MIN, SQB_MAX = 0, 1, 2
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+# Names of the functions include/sqdft_b200.h declares (checked by the tests).
+EXPORTS = [
+    "sqb_create", "sqb_destroy", "sqb_set_precision", "sqb_set_allreduce", "sqb_set_launch", "sqb_set_veff",
+    "sqb_set_atoms", "sqb_nonlocal_projectors", "sqb_set_projectors", "sqb_hsub_times_vec",
+    "sqb_lanczos_moments", "sqb_ne_constraint", "sqb_fermi_level", "sqb_density_energy",
+    "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
+]
+
+
+class SqbGrid(C.Structure):
+    _fields_ = [("np", C.c_int * 3), ("pnode_s", C.c_int * 3), ("n_int", C.c_int * 3), ("nloc", C.c_int),
+                ("fdn", C.c_int), ("npl", C.c_int), ("fermi_alg", C.c_int), ("delta", C.c_double),
+                ("bet", C.c_double), ("lanczos_tol", C.c_double), ("fermi_tol", C.c_double),
+                ("ncharge", C.c_double), ("coeff_lap", C.c_double * 8), ("coeff_grad", C.c_double * 8)]
+
+
+class SqbSpecies(C.Structure):
+    _fields_ = [("natm", C.c_int), ("lmax", C.c_int), ("lloc", C.c_int), ("nlocc", C.c_int), ("size", C.c_int),
+                ("rc", C.c_double), ("denom", C.c_double * 4), ("tables", _dp)]
+
+
+class SqbStats(C.Structure):
+    _fields_ = [("ms_lanczos_moments", C.c_double), ("ms_fermi", C.c_double), ("ms_density", C.c_double),
+                ("ms_forces", C.c_double), ("ms_projectors", C.c_double), ("matvecs", C.c_longlong),
+                ("lanczos_iters", C.c_longlong), ("window_points", C.c_longlong), ("proj_points", C.c_longlong),
+                ("fermi_iters", C.c_int), ("max_lanczos_iters", C.c_int), ("kernel_launches", C.c_int)]
+
+
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, _dp, C.c_int, C.c_int, C.c_void_p)
+
+
+class SQBError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        super().__init__(f"{where}: {status_string(code)} (status {code})")
+        self.code = code
+
+
+_LIB = None
+
+
+def library() -> C.CDLL:
+    """Load the CUDA library; raise if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"sqdft_b200 CUDA library not built: {LIB_PATH} (run python -m sqdft_b200.build)")
+        lib = C.CDLL(str(LIB_PATH))
+        P = C.c_void_p
+        lib.sqb_create.argtypes = [C.POINTER(SqbGrid), C.c_int, C.POINTER(P)]
+        lib.sqb_destroy.argtypes = [P]
+        lib.sqb_set_precision.argtypes = [P, C.c_int]
+        lib.sqb_set_allreduce.argtypes = [P, ALLREDUCE_FN, C.c_void_p]
+        lib.sqb_set_launch.argtypes = [P, C.c_int, C.c_int]
+        lib.sqb_set_veff.argtypes = [P, _dp]
+        lib.sqb_set_atoms.argtypes = [P, C.c_int, C.POINTER(SqbSpecies), C.c_int, _ip, _ip, _dp, C.c_int]
+        lib.sqb_nonlocal_projectors.argtypes = [P, _dp]
+        lib.sqb_set_projectors.argtypes = [P, _dp]
+        lib.sqb_hsub_times_vec.argtypes = [P, C.c_int, _ip, _dp, _dp]
+        lib.sqb_lanczos_moments.argtypes = [P, _dp, _dp, _dp, _ip, _dp, _dp]
+        lib.sqb_ne_constraint.argtypes = [P, C.c_double, _dp]
+        lib.sqb_fermi_level.argtypes = [P, C.c_int, C.c_double, _dp, _ip]
+        lib.sqb_density_energy.argtypes = [P, C.c_double, _dp, _dp, _dp, _dp]
+        lib.sqb_spectral_quadrature.argtypes = [P, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        lib.sqb_forces_nonlocal.argtypes = [P, _dp, _dp, _dp, _dp]
+        lib.sqb_get_stats.argtypes = [P, C.POINTER(SqbStats)]
+        lib.sqb_status_string.argtypes = [C.c_int]
+        lib.sqb_status_string.restype = C.c_char_p
+        lib.sqb_version.restype = C.c_char_p
+        _LIB = lib
+    return _LIB
+
+
+def status_string(code: int) -> str:
+    return library().sqb_status_string(code).decode()
+
+
+def _check(code: int, where: str) -> None:
+    if code != 0:
+        raise SQBError(code, where)
+
+
+def _d(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _i(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(_ip)
+
+
+class Context:
+    """One sqb_ctx: a processor block of the grid resident on one GPU."""
+
+    def __init__(self, case: Case, device: int = 0, precision: int = SQB_FP64, allreduce=None):
+        self.lib = library()
+        self.case = case
+        g = SqbGrid()
+        g.np[:] = list(case.np_)
+        g.pnode_s[:] = list(case.pnode_s)
+        g.n_int[:] = list(case.n_int)
+        g.nloc, g.fdn, g.npl, g.fermi_alg = case.nloc, case.fdn, case.npl, case.fermi_alg
+        g.delta, g.bet, g.lanczos_tol, g.fermi_tol, g.ncharge = (case.delta, case.bet, case.lanczos_tol,
+                                                                case.fermi_tol, case.ncharge)
+        for k in range(case.fdn + 1):
+            g.coeff_lap[k] = float(case.coeff_lap[k])
+            g.coeff_grad[k] = float(case.coeff_grad[k])
+        self.ptr = C.c_void_p()
+        _check(self.lib.sqb_create(C.byref(g), device, C.byref(self.ptr)), "sqb_create")
+        self._cb = None
+        if allreduce is not None:
+            self.set_allreduce(allreduce)
+        self.set_precision(precision)
+        self._keep = []
+        self.set_veff(case.veff)
+        self.set_atoms(case)
+
+    def close(self):
+        if self.ptr:
+            self.lib.sqb_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- set-up --------------------------------------------------------------
+    def set_precision(self, precision: int):
+        _check(self.lib.sqb_set_precision(self.ptr, precision), "sqb_set_precision")
+
+    def set_launch(self, ctas_per_sm: int = 0, cols_per_thread: int = 0):
+        _check(self.lib.sqb_set_launch(self.ptr, ctas_per_sm, cols_per_thread), "sqb_set_launch")
+
+    def set_allreduce(self, fn):
+        """fn(values: np.ndarray, op: int) -> None, reducing in place across ranks."""
+
+        def cb(ptr, count, op, user):
+            try:
+                arr = np.ctypeslib.as_array(ptr, shape=(count,))
+                fn(arr, op)
+                return 0
+            except Exception:  # reported to the library as a failed reduction
+                return 1
+
+        self._cb = ALLREDUCE_FN(cb)
+        _check(self.lib.sqb_set_allreduce(self.ptr, self._cb, None), "sqb_set_allreduce")
+
+    def set_veff(self, veff_ext: np.ndarray):
+        v = np.ascontiguousarray(veff_ext, np.float64)
+        _check(self.lib.sqb_set_veff(self.ptr, _d(v)), "sqb_set_veff")
+
+    def set_atoms(self, case: Case):
+        types = (SqbSpecies * max(1, len(case.types)))()
+        tabs = []
+        for k, t in enumerate(case.types):
+            tab = np.ascontiguousarray(t.tables, np.float64)
+            tabs.append(tab)
+            types[k].natm, types[k].lmax, types[k].lloc, types[k].nlocc = t.natm, t.lmax, t.lloc, t.nlocc
+            types[k].size = tab.shape[1]
+            types[k].rc = t.rc
+            types[k].denom[:] = [float(x) for x in t.denom]
+            types[k].tables = _d(tab)
+        rt = np.ascontiguousarray(case.rep_type, np.int32)
+        ra = np.ascontiguousarray(case.rep_atom, np.int32)
+        rx = np.ascontiguousarray(case.rep_xyz, np.float64)
+        _check(self.lib.sqb_set_atoms(self.ptr, len(case.types), types, len(rt), _i(rt), _i(ra), _d(rx), case.n_atm),
+               "sqb_set_atoms")
+        self._keep = tabs
+
+    def nonlocal_projectors(self, copy_out: bool = False) -> np.ndarray | None:
+        out = np.zeros(self.table_size()) if copy_out else None
+        _check(self.lib.sqb_nonlocal_projectors(self.ptr, _d(out)), "sqb_nonlocal_projectors")
+        return out
+
+    def set_projectors(self, udvtm: np.ndarray):
+        u = np.ascontiguousarray(udvtm, np.float64)
+        _check(self.lib.sqb_set_projectors(self.ptr, _d(u)), "sqb_set_projectors")
+
+    def table_size(self) -> int:
+        c = self.case
+        return int(sum(c.types[t].nproj * c.types[t].ball ** 3 for t in c.rep_type))
+
+    # -- kernels ---------------------------------------------------------------
+    def hsub_times_vec(self, nodes, vin: np.ndarray) -> np.ndarray:
+        nodes = np.ascontiguousarray(nodes, np.int32)
+        vin = np.ascontiguousarray(vin, np.float64).reshape(len(nodes), -1)
+        out = np.zeros_like(vin)
+        _check(self.lib.sqb_hsub_times_vec(self.ptr, len(nodes), _i(nodes), _d(vin), _d(out)), "sqb_hsub_times_vec")
+        return out
+
+    def lanczos_moments(self):
+        c = self.case
+        n = c.n_nodes
+        r = dict(chi=np.zeros(n), zee=np.zeros(n), rho_pj=np.zeros((n, c.npl + 1)),
+                 lanczos_iters=np.zeros(n, np.int32), lmin=np.zeros(n), lmax=np.zeros(n))
+        _check(self.lib.sqb_lanczos_moments(self.ptr, _d(r["chi"]), _d(r["zee"]), _d(r["rho_pj"]),
+                                            _i(r["lanczos_iters"]), _d(r["lmin"]), _d(r["lmax"])),
+               "sqb_lanczos_moments")
+        return r
+
+    def ne_constraint(self, lam: float) -> float:
+        v = C.c_double()
+        _check(self.lib.sqb_ne_constraint(self.ptr, lam, C.byref(v)), "sqb_ne_constraint")
+        return v.value
+
+    def fermi_level(self, scf_iter: int = 1, lambda_warm: float = 0.0):
+        lam, it = C.c_double(), C.c_int()
+        _check(self.lib.sqb_fermi_level(self.ptr, scf_iter, lambda_warm, C.byref(lam), C.byref(it)),
+               "sqb_fermi_level")
+        return lam.value, it.value
+
+    def density_energy(self, lam: float):
+        c = self.case
+        rho = np.zeros(c.n_nodes)
+        ci = np.zeros((c.n_nodes, c.npl + 1))
+        ebs, eent = C.c_double(), C.c_double()
+        _check(self.lib.sqb_density_energy(self.ptr, lam, _d(rho), _d(ci), C.byref(ebs), C.byref(eent)),
+               "sqb_density_energy")
+        return dict(rho=rho.reshape(c.np_[2], c.np_[1], c.np_[0]), Ci=ci, Ebs=ebs.value, Eent=eent.value)
+
+    def spectral_quadrature(self, scf_iter: int, lambda_f: float, outputs: bool = True):
+        """sqb_spectral_quadrature; with outputs=False only the scalars come back."""
+        c = self.case
+        n = c.n_nodes
+        lam = C.c_double(lambda_f)
+        ebs, eent = C.c_double(), C.c_double()
+        arr = {}
+        if outputs:
+            arr = dict(rho=np.zeros(n), rho_pj=np.zeros((n, c.npl + 1)), Ci=np.zeros((n, c.npl + 1)),
+                       chi=np.zeros(n), zee=np.zeros(n))
+        _check(self.lib.sqb_spectral_quadrature(self.ptr, scf_iter, C.byref(lam), _d(arr.get("rho")),
+                                                _d(arr.get("rho_pj")), _d(arr.get("Ci")), _d(arr.get("chi")),
+                                                _d(arr.get("zee")), C.byref(ebs), C.byref(eent)),
+               "sqb_spectral_quadrature")
+        if outputs:
+            arr["rho"] = arr["rho"].reshape(c.np_[2], c.np_[1], c.np_[0])
+        arr.update(lambda_f=lam.value, Ebs=ebs.value, Eent=eent.value)
+        return arr
+
+    def forces_nonlocal(self, chi=None, zee=None, ci=None) -> np.ndarray:
+        f = np.zeros((self.case.n_atm, 3))
+        args = [None, None, None]
+        if chi is not None:
+            args = [np.ascontiguousarray(chi, np.float64), np.ascontiguousarray(zee, np.float64),
+                    np.ascontiguousarray(ci, np.float64)]
+        _check(self.lib.sqb_forces_nonlocal(self.ptr, _d(args[0]), _d(args[1]), _d(args[2]), _d(f)),
+               "sqb_forces_nonlocal")
+        return f
+
+    def stats(self) -> dict:
+        s = SqbStats()
+        _check(self.lib.sqb_get_stats(self.ptr, C.byref(s)), "sqb_get_stats")
+        return {k: getattr(s, k) for k, _ in SqbStats._fields_}
+
+
+@dataclass
+class SQState:
+    """The DS_SQ fields of the SQ step (ds_sq.h:128-238) for one block."""
+
+    case: Case
+    lambda_f: float = 0.0
+    rho: np.ndarray | None = None
+    rho_pj: np.ndarray | None = None
+    Ci: np.ndarray | None = None
+    chi: np.ndarray | None = None
+    zee: np.ndarray | None = None
+    Ebs: float = 0.0
+    Eent: float = 0.0
+    fnloc: np.ndarray | None = None
+    UdVtm: np.ndarray | None = None
+    precision: int = SQB_FP64
+    device: int = 0
+    ctx: Context | None = field(default=None, repr=False)
+
+    def context(self) -> Context:
+        if self.ctx is None:
+            self.ctx = Context(self.case, self.device, self.precision)
+        return self.ctx
+
+
+def NonlocalProjectors(s: SQState) -> None:
+    """nonlocal.cpp:317-518: projector tables of every replica atom (on the GPU)."""
+    s.UdVtm = s.context().nonlocal_projectors(copy_out=True)
+
+
+def ClenshawCurtisSpectralQuadrature(s: SQState, scf_iter: int) -> None:
+    """sq.cpp:377-834: rho, rho_pj, Ci, chi, zee, lambda_f, Ebs, Eent."""
+    ctx = s.context()
+    if s.UdVtm is None:
+        NonlocalProjectors(s)
+    out = ctx.spectral_quadrature(scf_iter, s.lambda_f)
+    s.rho, s.rho_pj, s.Ci, s.chi, s.zee = out["rho"], out["rho_pj"], out["Ci"], out["chi"], out["zee"]
+    s.lambda_f, s.Ebs, s.Eent = out["lambda_f"], out["Ebs"], out["Eent"]
+
+
+def ForcesNonLocal(s: SQState) -> None:
+    """forces.cpp:318-578: fnloc[n_atm][3] from the state's chi, zee, Ci."""
+    s.fnloc = s.context().forces_nonlocal(s.chi, s.zee, s.Ci)

@@ -1,0 +1,117 @@
+"""CUDA path against the reference outputs and the oracle (needs a B200).
+
+Tolerances (FP64 path vs the reference FP64 path):
+  window matvec           1e-13 relative
+  chi, zee                1e-10 absolute (Lanczos tolerance is 1e-6; equal
+                          iteration counts keep them at rounding level)
+  rho                     |d rho|_inf <= 1e-10
+  Ebs, Eent per atom      1e-8 Ha/atom
+  nonlocal forces         1e-7 Ha/bohr
+FP32-mixed path vs the FP64 path: relative rho error <= 1e-6 (max-norm
+relative to max rho), forces <= 1e-4 Ha/bohr.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["tiny", "lihs", "mid"]
+
+
+def _ctx(case, precision=0):
+    from sqdft_b200 import sq
+
+    ctx = sq.Context(case, device=0, precision=precision)
+    ctx.set_projectors(case.udvtm)
+    return ctx
+
+
+@pytest.mark.parametrize("name", ["tiny", "lihs", "mid"])
+def test_hsub_times_vec(golden, name):
+    case, ref = golden(name)
+    with _ctx(case) as ctx:
+        out = ctx.hsub_times_vec(ref["hv_nodes"], ref["hv_in"])
+    for got, want in zip(out, ref["hv_out"]):
+        assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_spectral_quadrature_fp64(golden, name):
+    case, ref = golden(name)
+    n_atm = case.n_atm
+    with _ctx(case) as ctx:
+        m = ctx.lanczos_moments()
+        assert np.abs(m["chi"] - ref["chi"]).max() <= 1e-10
+        assert np.abs(m["zee"] - ref["zee"]).max() <= 1e-10
+        assert np.abs(m["rho_pj"] - ref["rho_pj"]).max() <= 1e-10 * np.abs(ref["rho_pj"]).max()
+        out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+        assert np.abs(out["rho"] - ref["rho"]).max() <= 1e-10
+        assert abs(out["lambda_f"] - ref["lambda_f"][0]) <= 1e-10
+        assert abs(out["Ebs"] - ref["Ebs"][0]) / n_atm <= 1e-8
+        assert abs(out["Eent"] - ref["Eent"][0]) / n_atm <= 1e-8
+        f = ctx.forces_nonlocal()
+        assert np.abs(f - ref["fnloc"]).max() <= 1e-7
+
+
+def test_results_al_fermi_level(golden):
+    """tests/Al/results_Al:82: first-SCF Fermi level 0.236781162275 Ha."""
+    case, ref = golden("al")
+    with _ctx(case) as ctx:
+        out = ctx.spectral_quadrature(1, 0.0)
+    assert round(out["lambda_f"], 12) == 0.236781162275
+    assert np.abs(out["rho"] - ref["rho"]).max() <= 1e-10
+
+
+def test_lanczos_iterations_match_oracle(golden):
+    from oracle.pyoracle import Oracle
+
+    case, _ = golden("lihs")
+    orc = Oracle(case).lanczos_moments()
+    with _ctx(case) as ctx:
+        m = ctx.lanczos_moments()
+    assert np.array_equal(m["lanczos_iters"], orc["lanczos_iters"])
+    assert np.abs(m["lmin"] - orc["lmin"]).max() <= 1e-10
+    assert np.abs(m["lmax"] - orc["lmax"]).max() <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["tiny", "mid"])
+def test_mixed_precision_budget(golden, name):
+    case, ref = golden(name)
+    with _ctx(case, precision=1) as ctx:
+        out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+        f = ctx.forces_nonlocal()
+    rel = np.abs(out["rho"] - ref["rho"]).max() / np.abs(ref["rho"]).max()
+    assert rel <= 1e-6, rel
+    assert np.abs(f - ref["fnloc"]).max() <= 1e-4
+
+
+def test_deterministic(golden):
+    case, _ = golden("tiny")
+    with _ctx(case) as ctx:
+        a = ctx.spectral_quadrature(1, 0.0)
+        b = ctx.spectral_quadrature(1, 0.0)
+    assert np.array_equal(a["rho"], b["rho"]) and a["lambda_f"] == b["lambda_f"]
+
+
+def test_newton_fermi_and_warm_bracket(golden):
+    """fermi_alg 2 (NewtonRaphson) and the scf_iter > 1 bracket of BrentsAlgorithm, vs the oracle."""
+    import dataclasses
+
+    from oracle.pyoracle import Oracle
+
+    case, _ = golden("tiny")
+    orc = Oracle(case)
+    m = orc.lanczos_moments()
+    lam_b, _ = orc.fermi_level(m, scf_iter=3, lambda_warm=0.3)
+    newton_case = dataclasses.replace(case, fermi_alg=2)
+    lam_n, _ = Oracle(newton_case).fermi_level(m, scf_iter=1)
+    with _ctx(case) as ctx:
+        ctx.lanczos_moments()
+        lam, _ = ctx.fermi_level(3, 0.3)
+        assert abs(lam - lam_b) <= 1e-10
+    with _ctx(newton_case) as ctx:
+        ctx.lanczos_moments()
+        lam, _ = ctx.fermi_level(1, 0.0)
+        assert abs(lam - lam_n) <= 1e-10
