@@ -117,7 +117,7 @@ int ensure_tmp(sqb_ctx *c, size_t bytes) {
 
 int choose_cols(const sqb_ctx *c) {
   if (c->cols > 0) return c->cols;
-  return 2;
+  return node_kernel_threads(c->n, 1) <= 1024 ? 1 : 2;
 }
 
 int ensure_scratch(sqb_ctx *c, int grid) {

@@ -1,8 +1,9 @@
 /* Single-process stand-in for the subset of MPI-3 that SQDFT uses.
  *
- * Test infrastructure only: it lets the reference SQDFT sources compile and
- * run as one rank so that their own FP64 spectral-quadrature path can serve as
- * the oracle for the GPU kernels.  With one rank every neighbour of the
+ * It lets the SQDFT sources compile and run as one rank where no MPI is
+ * installed: the drop-in build (reference host code + the GPU SQ path) and
+ * the oracle build of the reference use it.  With a real MPI, put its
+ * include directory first instead.  With one rank every neighbour of the
  * distributed-graph topologies (initialize.cpp:335,458) is rank 0 itself, so a
  * neighbourhood all-to-all copies send block k into receive block k (MPI's
  * in-order matching of repeated edges).  That turns the halo exchanges of

@@ -11,6 +11,7 @@ library is an error.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -19,7 +20,7 @@ import numpy as np
 from .case import Case
 
 HERE = Path(__file__).resolve().parent
-LIB_PATH = HERE / "_build" / "libsqdft_b200.so"
+LIB_PATH = Path(os.environ.get("SQDFT_B200_LIB", HERE / "_build" / "libsqdft_b200.so"))
 
 SQB_FP64 = 0
 SQB_FP32_MIXED = 1
