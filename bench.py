@@ -1,0 +1,326 @@
+"""SQ-step throughput of sqdft_b200 on B200 (grid nodes per second).
+
+One step is ClenshawCurtisSpectralQuadrature on the whole grid of a
+benchmark system: Lanczos bounds and Chebyshev moments of every node,
+Fermi-level solve, density and energies.  The default workload is the
+108-atom FCC Al cell (48^3 = 110,592 nodes, 31^3 truncation windows,
+Chebyshev order 96) with the reference's own first-SCF-iteration Veff.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2]
+                    [--precision fp64|mixed] [--impl ours|reference]
+
+value  nodes / (device time of the step), inputs resident in HBM
+e2e    nodes / (wall time of the C-ABI call with host buffers: Veff copied
+       in from pinned memory, rho, rho_pj, Ci, chi, zee copied out)
+With N > 1 (torchrun, NCCL), rank r owns a z-slab of the grid; the
+Fermi-level sums and energies are all-reduced through the library's hook.
+--impl reference times the reference SQDFT compiled from its sources
+(oracle/_ref/sqref_driver: its LanczosAlgorithm and HsubTimesVec per node)
+on a node sample across all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM = 6650.0
+
+
+def hbm_peak():
+    try:
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def slab(case, rank, ws):
+    """The z-slab of the grid that rank `rank` of `ws` owns (whole grid if ws = 1)."""
+    if ws == 1:
+        return case
+    import dataclasses
+
+    nz = case.n_int[2]
+    if nz % ws:
+        raise SystemExit(f"grid of {nz} planes does not split over {ws} ranks")
+    sz, z0 = nz // ws, rank * (nz // ws)
+    nl = case.nloc
+    full = case.veff_block
+    kz = (np.arange(z0 - nl, z0 + sz + nl)) % nz
+    ky = (np.arange(case.n_int[1] + 2 * nl) - nl) % case.n_int[1]
+    kx = (np.arange(case.n_int[0] + 2 * nl) - nl) % case.n_int[0]
+    veff = np.ascontiguousarray(full[np.ix_(kz, ky, kx)])
+    return dataclasses.replace(case, np_=(case.n_int[0], case.n_int[1], sz), pnode_s=(0, 0, z0), veff=veff)
+
+
+def algorithmic_bytes(stats, case, precision):
+    """Bytes per node-kernel launch by the roofline's accounting: per matvec
+    step n_w (3 s_v + s_V) plus the projector tables of every atom whose ball
+    meets the window, steps = Lanczos iterations + 1 + npl/2 per node."""
+    nw = stats["window_points"]
+    n = case.n_nodes
+    lz_steps = stats["lanczos_iters"] + n
+    ch_steps = n * (case.npl // 2)
+    sv = 8 if precision == 0 else 4
+    proj_lz = stats["proj_points"] - stats["proj_points_cheb"]
+    return (lz_steps * nw * 32 + proj_lz * 8) + (ch_steps * nw * 4 * sv + stats["proj_points_cheb"] * sv)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from sqdft_b200 import sq
+    from sqdft_b200.cases import load as load_named
+
+    rank, ws, local = dist_env()
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    case = load_named(args.config)
+    my = slab(case, rank, ws)
+    prec = sq.SQB_FP64 if args.precision == "fp64" else sq.SQB_FP32_MIXED
+
+    def allreduce(values, op):
+        t = torch.from_numpy(values.copy()).cuda()
+        dist.all_reduce(t, op={0: dist.ReduceOp.SUM, 1: dist.ReduceOp.MIN, 2: dist.ReduceOp.MAX}[op])
+        values[:] = t.cpu().numpy()
+
+    ctx = sq.Context(my, device=local, precision=prec, allreduce=allreduce if ws > 1 else None)
+    ctx.nonlocal_projectors()
+    n = my.n_nodes
+    K1 = my.npl + 1
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+    veff_host = pin(my.veff.shape)
+    veff_host[...] = my.veff
+    outs = dict(rho=pin((n,)), rho_pj=pin((n, K1)), Ci=pin((n, K1)), chi=pin((n,)), zee=pin((n,)))
+    flush = torch.empty(256 * 2**20, dtype=torch.uint8, device="cuda")
+
+    import ctypes as C
+
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+
+    def step():
+        flush.fill_(1)  # evict L2 (126 MB) between steps
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        ctx.set_veff(veff_host)
+        lamv = C.c_double(case.lambda_f)
+        ebs, eent = C.c_double(), C.c_double()
+        rc = ctx.lib.sqb_spectral_quadrature(ctx.ptr, 1, C.byref(lamv), dp(outs["rho"]), dp(outs["rho_pj"]),
+                                             dp(outs["Ci"]), dp(outs["chi"]), dp(outs["zee"]), C.byref(ebs),
+                                             C.byref(eent))
+        if rc:
+            raise sq.SQBError(rc, "sqb_spectral_quadrature")
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        st = ctx.stats()
+        dev_ms = st["ms_lanczos_moments"] + st["ms_fermi"] + st["ms_density"]
+        return wall, dev_ms, st, lamv.value
+
+    for _ in range(args.warmup):
+        step()
+    walls, devs, node_ms = [], [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            wall, dev_ms, st, lam = step()
+            walls.append(wall)
+            devs.append(dev_ms)
+            node_ms.append(st["ms_lanczos_moments"])
+    wall = float(np.mean(walls))
+    dev = float(np.mean(devs)) * 1e-3
+    kern = float(np.mean(node_ms)) * 1e-3
+    if ws > 1:
+        t = torch.tensor([wall, dev, kern], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall, dev, kern = t.tolist()
+    st = ctx.stats()
+    traffic_per_node_step = None
+    tr = ROOT / "profiles" / "node_kernel_traffic.json"
+    if tr.exists():
+        traffic_per_node_step = json.loads(tr.read_text()).get(args.precision)
+    abytes = algorithmic_bytes(st, my, prec)
+    peak, peak_kind = hbm_peak()
+    achieved = abytes / kern / 1e9
+    steps_local = st["lanczos_iters"] + n + n * (my.npl // 2)
+    res = None
+    if rank == 0:
+        nodes = case.n_nodes
+        h2d = my.veff.nbytes * ws
+        d2h = sum(a.nbytes for a in outs.values()) * ws
+        cpu = cpu_baseline(args) if (ws == 1 and not args.no_cpu) else None
+        res = {
+            "metric": "SQ grid nodes/s (FP64 SQ step: Lanczos + Chebyshev moments + Fermi level + density)"
+            if prec == 0 else "SQ grid nodes/s (FP32-mixed SQ step)",
+            "value": nodes / dev, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64" if prec == 0 else "f32-mixed", "data": "synthetic (seeded-Gaussian-displaced FCC Al; "
+            "reference first-SCF Veff)",
+            "config": {"workload": f"{args.config}: {case.n_int[0]}^3 grid, {nodes} nodes, {case.nw}^3 windows, "
+                       f"npl {case.npl}, {case.n_atm} atoms", "nodes": nodes, "window": case.nw, "npl": case.npl,
+                       "precision": args.precision, "parallelism": f"z-slabs x{ws}", "l2": "flushed (256 MB write) "
+                       "before every step"},
+            "e2e": {"value": nodes / wall, "unit": "nodes/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind,
+                         "traffic": (traffic_per_node_step * steps_local) if traffic_per_node_step else None,
+                         "algorithmic_bytes": abytes, "kernel": "node_kernel", "kernel_ms": kern * 1e3},
+            "gpu_launches": int(st["kernel_launches"]),
+            "clocks": clocks.summary(),
+            "lanczos_iters_per_node": st["lanczos_iters"] / n, "fermi_iters": st["fermi_iters"],
+            "lambda_f": lam,
+        }
+        if cpu:
+            res["cpu_baseline"] = cpu
+    ctx.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if res:
+        print(json.dumps(res), flush=True)
+
+
+def reference_rate(config: str, sample: int, threads: int):
+    """Nodes/s of the reference's per-node SQ work on a node sample."""
+    from sqdft_b200.case import read_container
+    from sqdft_b200.configs.gen_configs import write_system
+
+    drv = ROOT / "oracle" / "_ref" / "sqref_driver"
+    pot = ROOT / "oracle" / "_ref" / "pot"
+    if not drv.exists():
+        return None, "reference build missing (make -C oracle ref)"
+    with tempfile.TemporaryDirectory() as td:
+        run = write_system(config, Path(td))
+        for p in pot.glob("*.pot"):
+            (run / p.name).symlink_to(p)
+        out = Path(td) / "ref"
+        subprocess.run([str(drv), str(run), config, str(out), "--sample", str(sample), "--threads", str(threads)],
+                       check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        r = read_container(f"{out}_sample.sqc")
+    return sample / float(r["t_sample"][0]), None
+
+
+def cpu_baseline(args):
+    threads = os.cpu_count() or 1
+    sample = max(2 * threads, 16) if args.cpu_sample <= 0 else args.cpu_sample
+    rate, err = reference_rate(args.config, sample, threads)
+    if rate is None:
+        return {"value": None, "unit": "nodes/s", "cores": threads, "kind": "reference", "sample": err}
+    return {"value": rate, "unit": "nodes/s", "cores": threads, "kind": "reference",
+            "sample": f"{sample} nodes of {args.config} (reference LanczosAlgorithm + Chebyshev moment loop over "
+                      f"HsubTimesVec, g++ -O2), {threads} threads; Fermi solve and density excluded (<1% of the step)"}
+
+
+def run_reference(args):
+    rank, ws, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sample = max(2 * threads, 16) if args.cpu_sample <= 0 else args.cpu_sample
+    rates = []
+    for _ in range(args.warmup):
+        reference_rate(args.config, sample, threads)
+    for _ in range(args.steps):
+        rate, err = reference_rate(args.config, sample, threads)
+        if rate is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
+            return
+        rates.append(rate)
+    v = float(np.mean(rates))
+    desc = (f"{sample} nodes of {args.config} per step (reference LanczosAlgorithm + Chebyshev moment loop over "
+            f"HsubTimesVec, g++ -O2), {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": "SQ grid nodes/s (FP64 SQ step: Lanczos + Chebyshev moments + Fermi level + "
+        "density)", "value": v, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sample / v * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded-Gaussian-displaced FCC Al; reference first-SCF Veff)",
+        "config": {"workload": args.config, "precision": "fp64"},
+        "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": threads, "kind": "reference", "sample": desc},
+        "e2e": {"value": v, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -94,7 +94,9 @@ typedef struct sqb_stats {
   long long matvecs;         /* window matvecs in the last node kernel */
   long long lanczos_iters;   /* sum of Lanczos iterations over nodes */
   long long window_points;   /* (2nloc+1)^3 */
-  long long proj_points;     /* sum over nodes and matvecs of projector-ball points read (algorithmic) */
+  long long proj_points;     /* sum over nodes and matvec steps of the projector-ball points of the
+                                atoms meeting the window (n_proj * n_b per atom, algorithmic) */
+  long long proj_points_cheb; /* the same over the Chebyshev steps only */
   int fermi_iters;
   int max_lanczos_iters;
   int kernel_launches;       /* kernels launched by the last SQ or forces call */

@@ -14,19 +14,96 @@
 //   --no-forces      skip ForcesNonLocal
 //   --hv K           also apply HsubTimesVec to K seeded vectors at K nodes
 //   --nodes-only     stop after the SQ set-up (export the inputs only)
+//   --sample K       CPU baseline: time the reference's per-node work
+//                    (LanczosAlgorithm, sq.cpp:965, and the moment loop of
+//                    sq.cpp:564-655 over HsubTimesVec) on K nodes spread over
+//                    the block, on --threads T host threads; writes the
+//                    sampled chi, zee, rho_pj and the wall time
 // Writes <out_prefix>_in.sqc (inputs, incl. the reference's UdVtm tables) and
 // <out_prefix>_out.sqc (outputs and timings).
 #include <unistd.h>
 
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ds_sq.h"
 #include "func_sq.h"
 #include "../sqdft_b200/dropin/sq_export.h"
+
+// double*** window array as the reference allocates them (sq.cpp:496-517).
+static double ***new3(int n) {
+  double ***a = new double **[n];
+  for (int k = 0; k < n; k++) {
+    a[k] = new double *[n];
+    for (int j = 0; j < n; j++) a[k][j] = new double[n]();
+  }
+  return a;
+}
+static void del3(double ***a, int n) {
+  for (int k = 0; k < n; k++) {
+    for (int j = 0; j < n; j++) delete[] a[k][j];
+    delete[] a[k];
+  }
+  delete[] a;
+}
+
+// Per-node work of ClenshawCurtisSpectralQuadrature for one node with the
+// reference's own LanczosAlgorithm and HsubTimesVec; the moment loop restates
+// sq.cpp:566-655 with the same expressions.
+static void sample_node(DS_SQ *p, int nd, double *chi, double *zee, double *rpj) {
+  const int nl = p->nloc, n = 2 * nl + 1;
+  const int i = nd % p->np_x + nl, j = (nd / p->np_x) % p->np_y + nl, k = nd / (p->np_x * p->np_y) + nl;
+  double ***vec = new3(n), ***hv = new3(n), ***t0 = new3(n), ***t1 = new3(n), ***t2 = new3(n);
+  for (int a = 0; a < n; a++)
+    for (int b = 0; b < n; b++)
+      for (int c = 0; c < n; c++) vec[a][b][c] = 1.0;
+  double lmin, lmax;
+  LanczosAlgorithm(p, vec, i, j, k, &lmin, &lmax, nd + 1);
+  const double ch = (lmax + lmin) / 2, ze = (lmax - lmin) / 2;
+  *chi = ch;
+  *zee = ze;
+  const double h3 = pow(p->delta, 3);
+  for (int a = 0; a < n; a++)
+    for (int b = 0; b < n; b++)
+      for (int c = 0; c < n; c++) t0[a][b][c] = (a == nl && b == nl && c == nl) ? 1.0 : 0.0;
+  HsubTimesVec(p, t0, i, j, k, hv);
+  for (int a = 0; a < n; a++)
+    for (int b = 0; b < n; b++)
+      for (int c = 0; c < n; c++) t1[a][b][c] = (hv[a][b][c] - ch * t0[a][b][c]) / ze;
+  const double htemp = t1[nl][nl][nl];
+  const int q1 = (int)round(0.25 * p->npl), q2 = (int)round(0.5 * p->npl);
+  rpj[0] = t0[nl][nl][nl] / h3;
+  rpj[1] = t1[nl][nl][nl] / h3;
+  for (int nq = 2; nq <= q2; nq++) {
+    double d1 = 0.0, d2 = 0.0;
+    HsubTimesVec(p, t1, i, j, k, hv);
+    for (int a = 0; a < n; a++)
+      for (int b = 0; b < n; b++)
+        for (int c = 0; c < n; c++) {
+          t2[a][b][c] = (2 * (hv[a][b][c] - ch * t1[a][b][c]) / ze) - t0[a][b][c];
+          d1 += t2[a][b][c] * t2[a][b][c];
+          d2 += t2[a][b][c] * t1[a][b][c];
+          t0[a][b][c] = t1[a][b][c];
+          t1[a][b][c] = t2[a][b][c];
+        }
+    rpj[nq] = t2[nl][nl][nl] / h3;
+    if (nq > q1) {
+      rpj[2 * nq] = (2 * d1 - 1) / h3;
+      rpj[2 * nq - 1] = (2 * d2 - htemp) / h3;
+    }
+  }
+  del3(vec, n);
+  del3(hv, n);
+  del3(t0, n);
+  del3(t1, n);
+  del3(t2, n);
+}
 
 static unsigned long long lcg_state = 0x9E3779B97F4A7C15ull;
 static double lcg_uniform() {  // deterministic [-1, 1) values for the HsubTimesVec fixture
@@ -41,7 +118,7 @@ int main(int argc, char **argv) {
   }
   std::string run_dir = argv[1], stem = argv[2], out = argv[3];
   std::string veff_file;
-  int scf_iter = 1, hv_count = 0, do_forces = 1, nodes_only = 0;
+  int scf_iter = 1, hv_count = 0, do_forces = 1, nodes_only = 0, sample = 0, threads = 1;
   double lambda_warm = 0.0;
   int have_lambda = 0;
   for (int a = 4; a < argc; a++) {
@@ -51,6 +128,8 @@ int main(int argc, char **argv) {
     else if (!std::strcmp(argv[a], "--no-forces")) do_forces = 0;
     else if (!std::strcmp(argv[a], "--hv") && a + 1 < argc) hv_count = std::atoi(argv[++a]);
     else if (!std::strcmp(argv[a], "--nodes-only")) nodes_only = 1;
+    else if (!std::strcmp(argv[a], "--sample") && a + 1 < argc) sample = std::atoi(argv[++a]);
+    else if (!std::strcmp(argv[a], "--threads") && a + 1 < argc) threads = std::atoi(argv[++a]);
     else { std::fprintf(stderr, "unknown option %s\n", argv[a]); return 2; }
   }
   // Output paths are made absolute before changing into the run directory.
@@ -106,6 +185,41 @@ int main(int argc, char **argv) {
   }
   if (have_lambda) SQ.lambda_f = lambda_warm;
   const double lambda_in = SQ.lambda_f;
+
+  if (sample > 0) {
+    // Single rank: the Rcut halo of Veff is the periodic wrap of the block
+    // (what the exchange of sq.cpp:400-492 produces with one process).
+    const int ex = nx + 2 * nl, ey = ny + 2 * nl, ez = nz + 2 * nl;
+    for (int k = 0; k < ez; k++)
+      for (int j = 0; j < ey; j++)
+        for (int i = 0; i < ex; i++) {
+          const int kk = ((k - nl) % nz + nz) % nz, jj = ((j - nl) % ny + ny) % ny, ii = ((i - nl) % nx + nx) % nx;
+          SQ.Veff[k][j][i] = SQ.Veff[kk + nl][jj + nl][ii + nl];
+        }
+    if (sample > nnode) sample = nnode;
+    std::vector<int> nodes(sample);
+    for (int q = 0; q < sample; q++) nodes[q] = (int)(((long long)q * nnode) / sample + (nnode / sample) / 2) % nnode;
+    std::vector<double> chi(sample), zee(sample), rpj((size_t)sample * (SQ.npl + 1));
+    std::atomic<int> next(0);
+    auto t_start = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int t = 0; t < (threads > 0 ? threads : 1); t++)
+      pool.emplace_back([&]() {
+        for (int q; (q = next++) < sample;) sample_node(&SQ, nodes[q], &chi[q], &zee[q], &rpj[(size_t)q * (SQ.npl + 1)]);
+      });
+    for (auto &th : pool) th.join();
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    sqb::CaseWriter w(out + "_sample.sqc");
+    w.i32("sample_nodes", nodes.data(), {sample});
+    w.f64("sample_chi", chi.data(), {sample});
+    w.f64("sample_zee", zee.data(), {sample});
+    w.f64("sample_rho_pj", rpj.data(), {sample, SQ.npl + 1});
+    w.f64s("t_sample", secs);
+    w.i32s("threads", threads);
+    w.close();
+    std::printf("sqref_driver: %d nodes in %.3f s on %d threads\n", sample, secs, threads);
+    return 0;
+  }
 
   if (nodes_only) {
     // Only the block interior is valid here; the SQ call fills the halo.

@@ -183,7 +183,7 @@ int run_nodes(sqb_ctx *c, NodeArgs &a, const int *d_list, int count) {
   a.n_list = count;
   CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
-  CK(cudaMemsetAsync(c->d_proj_points, 0, sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->d_proj_points, 0, 2 * sizeof(unsigned long long), c->stream));
   CK(launch_node_kernel(a, grid, cols, c->stream));
   return SQB_OK;
 }
@@ -405,7 +405,7 @@ int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out) {
   const size_t N = c->nnode, K = g.npl + 1;
   CK(dalloc(&c->d_counter, 1));
   CK(dalloc(&c->d_status, 1));
-  CK(dalloc(&c->d_proj_points, 1));
+  CK(dalloc(&c->d_proj_points, 2));
   CK(dalloc(&c->d_nodes, N));
   CK(dalloc(&c->d_iters, N));
   CK(dalloc(&c->d_chi, N));
@@ -695,8 +695,8 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   const size_t N = c->nnode, K = c->g.npl + 1;
   std::vector<int> its(N);
   CK(cudaMemcpy(its.data(), c->d_iters, N * sizeof(int), cudaMemcpyDeviceToHost));
-  unsigned long long pp = 0;
-  CK(cudaMemcpy(&pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
+  unsigned long long pp[2] = {0, 0};
+  CK(cudaMemcpy(pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
   long long sum = 0;
   int mx = 0;
   for (size_t i = 0; i < N; i++) {
@@ -706,8 +706,9 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   c->stats.lanczos_iters = sum;
   c->stats.max_lanczos_iters = mx;
   // passes: Lanczos 2 per iteration + 2, Chebyshev npl/2 (matvec passes only)
-  c->stats.matvecs = (sum + 1) + (long long)N * (c->g.npl / 2);
-  c->stats.proj_points = (long long)pp;
+  c->stats.matvecs = sum + (long long)N + (long long)N * (c->g.npl / 2);
+  c->stats.proj_points = (long long)pp[0];
+  c->stats.proj_points_cheb = (long long)pp[1];
   if (lanczos_iters) std::memcpy(lanczos_iters, its.data(), N * sizeof(int));
   if (chi) CK(cudaMemcpy(chi, c->d_chi, N * sizeof(double), cudaMemcpyDeviceToHost));
   if (zee) CK(cudaMemcpy(zee, c->d_zee, N * sizeof(double), cudaMemcpyDeviceToHost));

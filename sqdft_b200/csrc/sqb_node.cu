@@ -500,11 +500,14 @@ __device__ __forceinline__ T *slot(const NodeArgs &a, int k) {
   return reinterpret_cast<T *>(a.scratch + blockIdx.x * a.scratch_stride + (size_t)k * nw * sizeof(double));
 }
 
-__device__ void count_proj_points(const NodeArgs &a, NodeShared &S, int passes) {
+// Projector-ball points of the boxes meeting this window times the matvec
+// steps taken: slot 0 all steps, slot 1 the Chebyshev steps only.
+__device__ void count_proj_points(const NodeArgs &a, NodeShared &S, int passes, int cheb) {
   if (threadIdx.x != 0 || a.proj_points == nullptr) return;
   unsigned long long s = 0;
   for (int e = 0; e < S.n_ent; e++) s += (unsigned long long)S.e_np[e] * S.e_nb[e];
   atomicAdd(a.proj_points, s * (unsigned long long)passes);
+  if (cheb) atomicAdd(a.proj_points + 1, s * (unsigned long long)passes);
 }
 
 // Lanczos bounds (FP64), sq.cpp:965-1092.
@@ -616,7 +619,7 @@ __device__ void lanczos(const NodeArgs &a, NodeShared &S, unsigned char *dyn, co
   lmin_out = S.eig[0] - a.lanczos_tol;
   lmax_out = S.eig[1] + a.lanczos_tol;
   iters = S.count;
-  count_proj_points(a, S, passes);
+  count_proj_points(a, S, S.count + 1, 0);  // Lanczos: iterations + the first matvec
 }
 
 // Chebyshev moments (sq.cpp:564-655) in precision T.
@@ -671,7 +674,7 @@ __device__ void moments(const NodeArgs &a, NodeShared &S, unsigned char *dyn, co
     t0 = t1;
     t1 = tt;
   }
-  count_proj_points(a, S, q2 + 1);
+  count_proj_points(a, S, q2, 1);  // Chebyshev: npl/2 matvecs
 }
 
 // ForcesNonLocal for one node (forces.cpp:318-578).
@@ -776,7 +779,7 @@ __device__ void node_forces(const NodeArgs &a, NodeShared &S, unsigned char *dyn
     slotc++;
     __syncthreads();
   }
-  count_proj_points(a, S, a.npl + 1);
+  count_proj_points(a, S, a.npl, 1);
 }
 
 template <int C>

@@ -54,6 +54,7 @@ class SqbStats(C.Structure):
     _fields_ = [("ms_lanczos_moments", C.c_double), ("ms_fermi", C.c_double), ("ms_density", C.c_double),
                 ("ms_forces", C.c_double), ("ms_projectors", C.c_double), ("matvecs", C.c_longlong),
                 ("lanczos_iters", C.c_longlong), ("window_points", C.c_longlong), ("proj_points", C.c_longlong),
+                ("proj_points_cheb", C.c_longlong),
                 ("fermi_iters", C.c_int), ("max_lanczos_iters", C.c_int), ("kernel_launches", C.c_int)]
 
 
