@@ -161,6 +161,32 @@ int sqb_spectral_quadrature(sqb_ctx *ctx, int scf_iter, double *lambda_f, double
  * sqb_spectral_quadrature call (or given ones when not NULL). */
 int sqb_forces_nonlocal(sqb_ctx *ctx, const double *chi, const double *zee, const double *ci, double *forces);
 
+/* Size of the fixed device scratch array used by sqb_lanczos_moments_noalloc
+ * (held on every GPU that loads the library, until the process exits). */
+#define SQB_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* sqb_lanczos_moments without any GPU allocation during the call, for callers
+ * that may not allocate device memory while they run: code inside an
+ * allocator-managed framework that owns all device memory, or a host loop
+ * that has to keep its memory footprint fixed.  No counterpart in the
+ * reference.
+ *
+ * It runs the same node kernel as sqb_lanczos_moments for the `count` block
+ * nodes listed in host array `nodes`, but the kernel's per-CTA window
+ * vectors, its work-queue counter and status word live in one fixed device
+ * array of SQB_NOALLOC_SCRATCH_BYTES compiled into the library, not in
+ * memory from cudaMalloc.  Inputs are the context's resident Veff, atoms and
+ * projector tables; outputs go to caller-owned DEVICE arrays indexed by node
+ * id (chi, zee: nnode doubles; rho_pj: nnode x (npl+1); lanczos_iters may be
+ * NULL).  The call is synchronous and returns a status code; a window whose
+ * scratch (plus the node list) does not fit the array is rejected with
+ * SQB_ERR_CAPACITY.  The first call on a device looks up the array's device
+ * address for that device, so make it before any stream capture.  All calls
+ * in the process share the array: calls that overlap on the GPU (other
+ * threads or streams) race and must be serialised by the caller. */
+int sqb_lanczos_moments_noalloc(sqb_ctx *ctx, int count, const int *nodes, double *d_chi, double *d_zee,
+                                double *d_rho_pj, int *d_lanczos_iters);
+
 int sqb_get_stats(const sqb_ctx *ctx, sqb_stats *out);
 const char *sqb_status_string(int status);
 /* Library version string. */

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/sqdft_b200.h"
@@ -818,6 +819,87 @@ int sqb_forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const 
   if (rc) return rc;
   if (c->n_atm > 0) CK(cudaMemcpy(forces, c->d_f, (size_t)3 * c->n_atm * sizeof(double), cudaMemcpyDeviceToHost));
   return reduce(c, forces, 3 * c->n_atm, SQB_SUM);
+}
+
+// Fixed scratch of sqb_lanczos_moments_noalloc: header (work-queue counter,
+// status word), then the node list, then the per-CTA window slots.  Host code
+// must not pass this symbol to a kernel: its device address comes from
+// cudaGetSymbolAddress, looked up once per device with that device current.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SQB_NOALLOC_SCRATCH_BYTES];
+static void *g_noalloc_addr[256];
+static std::mutex g_noalloc_mu;
+
+static int noalloc_base(int device, unsigned char **base) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (device < 0 || device >= 256) return SQB_ERR_ARG;
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      std::fprintf(stderr, "sqdft_b200: cudaGetSymbolAddress of the no-alloc scratch: %s\n", cudaGetErrorString(e));
+      return SQB_ERR_CUDA;
+    }
+    g_noalloc_addr[device] = p;
+  }
+  *base = static_cast<unsigned char *>(g_noalloc_addr[device]);
+  return SQB_OK;
+}
+
+int sqb_lanczos_moments_noalloc(sqb_ctx *c, int count, const int *nodes, double *d_chi, double *d_zee,
+                                double *d_rho_pj, int *d_lanczos_iters) {
+  if (!c || count < 0 || (count > 0 && (!nodes || !d_chi || !d_zee || !d_rho_pj))) return SQB_ERR_ARG;
+  if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
+  if (count == 0) return SQB_OK;
+  for (int i = 0; i < count; i++)
+    if (nodes[i] < 0 || nodes[i] >= c->nnode) return SQB_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  const size_t nw = (size_t)c->n * c->n * c->n;
+  const size_t stride = ((4 * nw * sizeof(double)) + 255) & ~size_t(255);
+  const size_t header = 256, list_bytes = ((size_t)count * sizeof(int) + 255) & ~size_t(255);
+  if (header + list_bytes + stride > SQB_NOALLOC_SCRATCH_BYTES) {
+    std::fprintf(stderr,
+                 "sqdft_b200: sqb_lanczos_moments_noalloc needs %zu bytes of scratch for one CTA and %d nodes; "
+                 "the fixed array holds %u\n",
+                 header + list_bytes + stride, count, SQB_NOALLOC_SCRATCH_BYTES);
+    return SQB_ERR_CAPACITY;
+  }
+  unsigned char *base = nullptr;
+  int rc = noalloc_base(c->device, &base);
+  if (rc) return rc;
+  const int cols = choose_cols(c);
+  if (node_kernel_threads(c->n, cols) > 1024) return SQB_ERR_UNSUPPORTED;
+  int grid = c->sms * (c->ctas_per_sm > 0 ? c->ctas_per_sm : 1);
+  const size_t fit = (SQB_NOALLOC_SCRATCH_BYTES - header - list_bytes) / stride;
+  if ((size_t)grid > fit) grid = (int)fit;
+  if (grid > count) grid = count;
+  int *d_counter = reinterpret_cast<int *>(base);
+  int *d_status = reinterpret_cast<int *>(base + 64);
+  int *d_list = reinterpret_cast<int *>(base + header);
+  NodeArgs a;
+  fill_node_args(c, a);
+  a.mode = MODE_SQ;
+  a.chi = d_chi;
+  a.zee = d_zee;
+  a.rho_pj = d_rho_pj;
+  a.lmin = nullptr;
+  a.lmax = nullptr;
+  a.lanczos_iters = d_lanczos_iters;
+  a.counter = d_counter;
+  a.status = d_status;
+  a.proj_points = nullptr;
+  a.scratch = base + header + list_bytes;
+  a.scratch_stride = stride;
+  a.node_list = d_list;
+  a.n_list = count;
+  // The array keeps the previous call's contents: the counter and status
+  // start at zero, the node list is written; window slots need no clearing.
+  CK(cudaMemsetAsync(base, 0, header, c->stream));
+  CK(cudaMemcpyAsync(d_list, nodes, (size_t)count * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_node_kernel(a, grid, cols, c->stream));
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return status_to_err(st);
 }
 
 int sqb_get_stats(const sqb_ctx *c, sqb_stats *out) {

@@ -35,6 +35,7 @@ EXPORTS = [
     "sqb_set_atoms", "sqb_nonlocal_projectors", "sqb_set_projectors", "sqb_hsub_times_vec",
     "sqb_lanczos_moments", "sqb_ne_constraint", "sqb_fermi_level", "sqb_density_energy",
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
+    "sqb_lanczos_moments_noalloc",
 ]
 
 
@@ -95,6 +96,7 @@ def library() -> C.CDLL:
         lib.sqb_spectral_quadrature.argtypes = [P, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         lib.sqb_forces_nonlocal.argtypes = [P, _dp, _dp, _dp, _dp]
         lib.sqb_get_stats.argtypes = [P, C.POINTER(SqbStats)]
+        lib.sqb_lanczos_moments_noalloc.argtypes = [P, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
         lib.sqb_version.restype = C.c_char_p

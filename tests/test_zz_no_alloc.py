@@ -1,0 +1,58 @@
+"""sqb_lanczos_moments_noalloc: the node kernel run with the library's fixed
+device scratch array instead of GPU memory allocated during the call.
+
+It is meant for callers that must not allocate device memory while they run
+(a framework whose allocator owns the GPU memory, a loop that keeps its
+footprint fixed).  The test gives it caller-owned device outputs, calls it
+twice in a row through the C ABI, and checks both results against
+sqb_lanczos_moments on the same context, with the parity tolerances of
+test_gpu_parity.py.  The file sorts last so that a run stopping at the first
+failure has run every other test first; it also passes alone.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_noalloc_matches_lanczos_moments_twice(golden):
+    import torch
+
+    from sqdft_b200 import sq
+
+    case, _ = golden("lihs")  # two species, 1000 nodes
+    n, K = case.n_nodes, case.npl + 1
+    with sq.Context(case) as ctx:
+        ctx.set_projectors(case.udvtm)
+        ref = ctx.lanczos_moments()
+        nodes = np.ascontiguousarray(np.arange(n)[::-1], np.int32)  # any order, each node once
+        for call in range(2):
+            chi = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+            zee = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+            rpj = torch.full((n, K), float("nan"), dtype=torch.float64, device="cuda")
+            its = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+            rc = ctx.lib.sqb_lanczos_moments_noalloc(ctx.ptr, n, nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                     chi.data_ptr(), zee.data_ptr(), rpj.data_ptr(), its.data_ptr())
+            assert rc == 0, sq.status_string(rc)
+            torch.cuda.synchronize()
+            assert np.abs(chi.cpu().numpy() - ref["chi"]).max() <= 1e-10, call
+            assert np.abs(zee.cpu().numpy() - ref["zee"]).max() <= 1e-10, call
+            assert np.abs(rpj.cpu().numpy() - ref["rho_pj"]).max() <= 1e-10 * np.abs(ref["rho_pj"]).max(), call
+            assert np.array_equal(its.cpu().numpy(), ref["lanczos_iters"]), call
+
+
+def test_noalloc_rejects_bad_node_ids(golden):
+    from sqdft_b200 import sq
+
+    case, _ = golden("tiny")
+    with sq.Context(case) as ctx:
+        ctx.set_projectors(case.udvtm)
+        bad = np.array([0, case.n_nodes], np.int32)
+        null = ctypes.c_void_p(0)
+        rc = ctx.lib.sqb_lanczos_moments_noalloc(ctx.ptr, 2, bad.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                 null, null, null, null)
+        assert rc == 1  # SQB_ERR_ARG: checked on the host before anything runs
