@@ -219,10 +219,12 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
     ld_point(c, 0);
   }
 
-  T cl[FDN + 1];
-#pragma unroll
-  for (int k = 0; k <= FDN; k++) cl[k] = (T)a.coeff_lap[k];
-  const T chi = (T)io.ca, zee = (T)io.cb;
+  // Arithmetic is FP64 for both storage types: with FP32 storage (mixed
+  // path) the six neighbour pairs of each stencil arm are summed in FP32 and
+  // everything after that -- the 7-term stencil sum, Veff, the nonlocal
+  // gather and the recursion update -- in FP64, so the rounding left is the
+  // FP32 storage of the vectors.
+  const double chi = io.ca, zee = io.cb;
 
   for (int z = 0; z <= n; z++) {
     T *smz = sm_in + (z & 1) * P2;
@@ -239,17 +241,17 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
     for (int c = 0; c < C; c++) {
       if (!ok[c]) continue;
       const size_t g = (size_t)z * n2 + col[c];
-      T hv = T(0), v = T(0);
+      double hv = 0.0, v = 0.0;
       if constexpr (STENCIL) {
-        v = win[c][FDN];
+        v = (double)win[c][FDN];
         const int idx = (cy[c] + FDN) * P + cx[c] + FDN;
-        T temp = v * T(3) * cl[0];
+        double temp = v * 3.0 * a.coeff_lap[0];
 #pragma unroll
         for (int k = 1; k <= FDN; k++) {
           T s = smz[idx - k] + smz[idx + k] + smz[idx - k * P] + smz[idx + k * P] + win[c][FDN - k] + win[c][FDN + k];
-          temp += s * cl[k];
+          temp += (double)s * a.coeff_lap[k];
         }
-        T vnl = T(0);
+        double vnl = 0.0;
 #pragma unroll
         for (int w = 0; w < 4; w++) {
           uint32_t m = mask[c][w];
@@ -260,10 +262,10 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
             const int Sd = S.e_S[e];
             const T *U = tab + S.e_tab[e] + S.e_base[e] + (z * Sd + cy[c]) * Sd + cx[c];
             const int pb = S.e_pb[e], np = S.e_np[e], nb = S.e_nb[e];
-            for (int q = 0; q < np; q++) vnl += (T)S.p_cur[pb + q] * U[(long long)q * nb];
+            for (int q = 0; q < np; q++) vnl += S.p_cur[pb + q] * (double)U[(long long)q * nb];
           }
         }
-        hv = T(-0.5) * temp + q_ve[c] * v + vnl;
+        hv = -0.5 * temp + (double)q_ve[c] * v + vnl;
       }
       T o = T(0);
       if constexpr (PK == PK_ONES) {
@@ -275,28 +277,29 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
       } else if constexpr (PK == PK_DOTS) {
         o = pf[c];
       } else if constexpr (PK == PK_HV) {
-        o = hv;
+        o = (T)hv;
         io.out[g] = o;
-        acc0 += (double)v * (double)hv;
+        acc0 += v * hv;
       } else if constexpr (PK == PK_LZB) {
         o = q_p1[c] - (T)io.ca * pf[c] - (T)io.cb * q_p2[c];
         io.out[g] = o;
         acc0 += (double)o * (double)o;
       } else if constexpr (PK == PK_CH1) {
-        o = (hv - chi * v) / zee;
+        o = (T)((hv - chi * v) / zee);
         io.out[g] = o;
       } else if constexpr (PK == PK_CH || PK == PK_FD) {
-        o = (T(2) * (hv - chi * v)) / zee - q_p1[c];
+        const double od = (2.0 * (hv - chi * v)) / zee - (double)q_p1[c];
+        o = (T)od;
         io.out[g] = o;
         if (io.dbl) {
           acc0 += (double)o * (double)o;
-          acc1 += (double)o * (double)v;
+          acc1 += (double)o * v;
         }
         if constexpr (PK == PK_FD) io.dacc[g] = q_d[c] + (double)o * io.cd / a.h3;
       } else if constexpr (PK == PK_FD01) {
         io.dacc[g] = 0.0 + (double)q_p1[c] * io.cd / a.h3 + (double)q_p2[c] * io.ce / a.h3;
       } else if constexpr (PK == PK_APPLY) {
-        io.dout[g] = (double)hv;
+        io.dout[g] = hv;
       }
       if constexpr (DOTS) smo[col[c]] = o;
       if (col[c] == centre_col && z == a.nloc) S.center_val = (double)o;
@@ -783,7 +786,7 @@ __device__ void node_forces(const NodeArgs &a, NodeShared &S, unsigned char *dyn
 }
 
 template <int C>
-__global__ void __launch_bounds__(C == 1 ? 1024 : 640, 1) node_kernel(NodeArgs a) {
+__global__ void __launch_bounds__(C == 1 ? 1024 : 576, 1) node_kernel(NodeArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   NodeShared &S = *reinterpret_cast<NodeShared *>(smem);
   unsigned char *dyn = smem + kSharedFixed;
