@@ -97,25 +97,6 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def slab(case, rank, ws):
-    """The z-slab of the grid that rank `rank` of `ws` owns (whole grid if ws = 1)."""
-    if ws == 1:
-        return case
-    import dataclasses
-
-    nz = case.n_int[2]
-    if nz % ws:
-        raise SystemExit(f"grid of {nz} planes does not split over {ws} ranks")
-    sz, z0 = nz // ws, rank * (nz // ws)
-    nl = case.nloc
-    full = case.veff_block
-    kz = (np.arange(z0 - nl, z0 + sz + nl)) % nz
-    ky = (np.arange(case.n_int[1] + 2 * nl) - nl) % case.n_int[1]
-    kx = (np.arange(case.n_int[0] + 2 * nl) - nl) % case.n_int[0]
-    veff = np.ascontiguousarray(full[np.ix_(kz, ky, kx)])
-    return dataclasses.replace(case, np_=(case.n_int[0], case.n_int[1], sz), pnode_s=(0, 0, z0), veff=veff)
-
-
 def algorithmic_bytes(stats, case, precision):
     """Bytes per node-kernel launch by the roofline's accounting: per matvec
     step n_w (3 s_v + s_V) plus the projector tables of every atom whose ball
@@ -135,6 +116,7 @@ def run_ours(args):
 
     from sqdft_b200 import sq
     from sqdft_b200.cases import load as load_named
+    from sqdft_b200.dist import allreduce_fn, slab
 
     rank, ws, local = dist_env()
     if ws > 1:
@@ -144,12 +126,7 @@ def run_ours(args):
     my = slab(case, rank, ws)
     prec = sq.SQB_FP64 if args.precision == "fp64" else sq.SQB_FP32_MIXED
 
-    def allreduce(values, op):
-        t = torch.from_numpy(values.copy()).cuda()
-        dist.all_reduce(t, op={0: dist.ReduceOp.SUM, 1: dist.ReduceOp.MIN, 2: dist.ReduceOp.MAX}[op])
-        values[:] = t.cpu().numpy()
-
-    ctx = sq.Context(my, device=local, precision=prec, allreduce=allreduce if ws > 1 else None)
+    ctx = sq.Context(my, device=local, precision=prec, allreduce=allreduce_fn(dist, "cuda") if ws > 1 else None)
     ctx.nonlocal_projectors()
     n = my.n_nodes
     K1 = my.npl + 1
