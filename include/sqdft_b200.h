@@ -19,6 +19,8 @@
 #ifndef SQDFT_B200_H
 #define SQDFT_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -108,7 +110,8 @@ int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out);
 int sqb_destroy(sqb_ctx *ctx);
 int sqb_set_precision(sqb_ctx *ctx, int precision);
 int sqb_set_allreduce(sqb_ctx *ctx, sqb_allreduce_fn fn, void *user);
-/* Nodes processed per persistent CTA batch and CTAs per SM (0 = automatic). */
+/* Launch shape of the node kernel: persistent CTAs per SM and window columns
+ * per thread (1 or 2).  0 for either = automatic. */
 int sqb_set_launch(sqb_ctx *ctx, int ctas_per_sm, int cols_per_thread);
 
 /* Veff on the block with its Rcut halo: the state of DS_SQ::Veff after the
@@ -187,7 +190,10 @@ int sqb_forces_nonlocal(sqb_ctx *ctx, const double *chi, const double *zee, cons
 int sqb_lanczos_moments_noalloc(sqb_ctx *ctx, int count, const int *nodes, double *d_chi, double *d_zee,
                                 double *d_rho_pj, int *d_lanczos_iters);
 
-int sqb_get_stats(const sqb_ctx *ctx, sqb_stats *out);
+/* Counters and timings of the last calls.  out_size is sizeof(sqb_stats) as
+ * the caller was compiled: the library writes min(out_size, its own size)
+ * bytes, so a caller built against an older, shorter sqb_stats stays safe. */
+int sqb_get_stats(const sqb_ctx *ctx, sqb_stats *out, size_t out_size);
 const char *sqb_status_string(int status);
 /* Library version string. */
 const char *sqb_version(void);

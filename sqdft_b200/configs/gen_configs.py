@@ -42,6 +42,7 @@ class System:
     basis: list[tuple[str, tuple[float, float, float]]]
     max_md: int = 1
     note: str = ""
+    xyz: tuple | None = None  # explicit Cartesian positions (bohr), in basis order
 
     @property
     def domain(self) -> float:
@@ -73,11 +74,21 @@ SYSTEMS = {
     "c4": System("c4", 7.78, 2, 16, 5.0, 64, 6.0, 0.05, 4, _al_basis(), note="FCC Al 32 atoms, 32^3"),
     "c5": System("c5", 7.78, 5, 16, 10.0, 128, 7.0, 0.05, 5, _al_basis(), max_md=10,
                  note="FCC Al 500 atoms, 80^3, NVE"),
+    # The reference's regression system tests/Al (test_Al.input, Al_eq.atoms):
+    # 4 Al atoms, one displaced, 10^3 grid, T = 46418.02 K, npl 28, Rcut 6.
+    "al_ref": System("al_ref", 7.78, 1, 10, 46418.02 * KB_EV, 28, 6.0, 0.0, 0, _al_basis(),
+                     note="reference regression Al, 4 atoms, 17^3 window",
+                     xyz=((0.0, 0.0, 0.0), (0.0, 3.89, 3.89), (3.89, 0.0, 3.89), (3.74, 3.49, 0.37))),
 }
 
 
 def positions(s: System) -> dict[str, np.ndarray]:
     """Cartesian positions per species: lattice sites plus seeded Gaussian noise, wrapped."""
+    if s.xyz is not None:
+        per: dict[str, list] = {}
+        for (sym, _), xyz in zip(s.basis, s.xyz):
+            per.setdefault(sym, []).append(xyz)
+        return {sym: np.array(v, dtype=float) for sym, v in per.items()}
     rng = np.random.default_rng(s.seed)
     per: dict[str, list] = {}
     for cz in range(s.cells):

@@ -902,9 +902,9 @@ int sqb_lanczos_moments_noalloc(sqb_ctx *c, int count, const int *nodes, double 
   return status_to_err(st);
 }
 
-int sqb_get_stats(const sqb_ctx *c, sqb_stats *out) {
-  if (!c || !out) return SQB_ERR_ARG;
-  *out = c->stats;
+int sqb_get_stats(const sqb_ctx *c, sqb_stats *out, size_t out_size) {
+  if (!c || !out || out_size == 0) return SQB_ERR_ARG;
+  std::memcpy(out, &c->stats, out_size < sizeof(sqb_stats) ? out_size : sizeof(sqb_stats));
   return SQB_OK;
 }
 

@@ -228,7 +228,7 @@ void ClenshawCurtisSpectralQuadrature(DS_SQ *p, int scf_iter) {
   p->Ebs = ebs;
   p->Eent = eent;
   sqb_stats st;
-  sqb_get_stats(g_ctx, &st);
+  sqb_get_stats(g_ctx, &st, sizeof(st));
   if (rank == 0) {
     std::printf("Lanczos took %d iterations (max over nodes, GPU). \n", st.max_lanczos_iters);
     std::printf("Brent's algorithm took %d iterations. \n", st.fermi_iters);

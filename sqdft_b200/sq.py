@@ -95,7 +95,7 @@ def library() -> C.CDLL:
         lib.sqb_density_energy.argtypes = [P, C.c_double, _dp, _dp, _dp, _dp]
         lib.sqb_spectral_quadrature.argtypes = [P, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         lib.sqb_forces_nonlocal.argtypes = [P, _dp, _dp, _dp, _dp]
-        lib.sqb_get_stats.argtypes = [P, C.POINTER(SqbStats)]
+        lib.sqb_get_stats.argtypes = [P, C.POINTER(SqbStats), C.c_size_t]
         lib.sqb_lanczos_moments_noalloc.argtypes = [P, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
@@ -289,7 +289,7 @@ class Context:
 
     def stats(self) -> dict:
         s = SqbStats()
-        _check(self.lib.sqb_get_stats(self.ptr, C.byref(s)), "sqb_get_stats")
+        _check(self.lib.sqb_get_stats(self.ptr, C.byref(s), C.sizeof(s)), "sqb_get_stats")
         return {k: getattr(s, k) for k, _ in SqbStats._fields_}
 
 
