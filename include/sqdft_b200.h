@@ -110,8 +110,10 @@ int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out);
 int sqb_destroy(sqb_ctx *ctx);
 int sqb_set_precision(sqb_ctx *ctx, int precision);
 int sqb_set_allreduce(sqb_ctx *ctx, sqb_allreduce_fn fn, void *user);
-/* Launch shape of the node kernel: persistent CTAs per SM and window columns
- * per thread (1 or 2).  0 for either = automatic. */
+/* Launch shape of the node kernel: persistent CTAs per SM, and the layout of
+ * its plane loop: window columns per thread (1 or 2; 0 = automatic, one
+ * column per thread when the window has at most 1024 columns), or -2 for the
+ * row layout (a warp per two window rows, windows up to 32 wide). */
 int sqb_set_launch(sqb_ctx *ctx, int ctas_per_sm, int cols_per_thread);
 
 /* Veff on the block with its Rcut halo: the state of DS_SQ::Veff after the

@@ -45,7 +45,10 @@ struct sqb_ctx {
   bool have_tables = false;
   double *d_tab64 = nullptr;
   float *d_tab32 = nullptr;
-  long long tab_total = 0;
+  long long tab_total = 0;      // values of the reference's UdVtm
+  long long tab_pad_total = 0;  // values of the padded device tables
+  long long *d_rep_off_ref = nullptr;
+  long long stage_elems = 0;  // largest per-plane projector-slice footprint (values)
   bool have_atoms = false, have_proj = false;
 
   unsigned char *d_scratch = nullptr;
@@ -104,6 +107,7 @@ int status_to_err(int st) {
   if (st & ST_SPLINE_RANGE) return SQB_ERR_SPLINE_RANGE;
   if (st & ST_NONFINITE) return SQB_ERR_NONFINITE;
   if (st & ST_LANCZOS_MAXITER) return SQB_ERR_LANCZOS_MAXITER;
+  if (st & ST_WAIT_LIMIT) return SQB_ERR_CUDA;
   return SQB_OK;
 }
 
@@ -116,10 +120,8 @@ int ensure_tmp(sqb_ctx *c, size_t bytes) {
   return SQB_OK;
 }
 
-int choose_cols(const sqb_ctx *c) {
-  if (c->cols > 0) return c->cols;
-  return node_kernel_threads(c->n, 1) <= 1024 ? 1 : 2;
-}
+// Columns per thread of the node kernel: 0 lets the launcher pick its layout.
+int choose_cols(const sqb_ctx *c) { return c->cols; }
 
 int ensure_scratch(sqb_ctx *c, int grid) {
   const size_t nw = (size_t)c->n * c->n * c->n;
@@ -166,6 +168,7 @@ void fill_node_args(sqb_ctx *c, NodeArgs &a) {
   a.status = c->d_status;
   a.mixed = c->precision == SQB_FP32_MIXED;
   a.proj_points = c->d_proj_points;
+  a.stage_bytes = node_kernel_stage_bytes(c->n, c->stage_elems);
 }
 
 // Launch the node kernel over `count` nodes of d_list; returns SQB status.
@@ -443,7 +446,7 @@ int sqb_destroy(sqb_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void *ptrs[] = {c->d_veff64, c->d_veff32, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
                   c->d_typ_nlocc, c->d_typ_nproj, c->d_typ_lmax, c->d_typ_lloc, c->d_typ_size, c->d_proj_denom,
-                  c->d_tables, c->d_rep_xyz, c->d_tab64, c->d_tab32, c->d_scratch, c->d_counter, c->d_nodes,
+                  c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_tab64, c->d_tab32, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
                   c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
                   c->d_f, c->d_tmp};
@@ -470,7 +473,10 @@ int sqb_set_allreduce(sqb_ctx *c, sqb_allreduce_fn fn, void *user) {
 }
 
 int sqb_set_launch(sqb_ctx *c, int ctas_per_sm, int cols_per_thread) {
-  if (!c || ctas_per_sm < 0 || ctas_per_sm > 4 || cols_per_thread < 0 || cols_per_thread > 2) return SQB_ERR_ARG;
+  if (!c || ctas_per_sm < 0 || ctas_per_sm > 4 || cols_per_thread < -2 || cols_per_thread > 2 ||
+      cols_per_thread == -1)
+    return SQB_ERR_ARG;
+  if (cols_per_thread == -2 && c->n > 32) return SQB_ERR_UNSUPPORTED;
   if (cols_per_thread > 0 && node_kernel_threads(c->n, cols_per_thread) > 1024) return SQB_ERR_UNSUPPORTED;
   c->ctas_per_sm = ctas_per_sm > 0 ? ctas_per_sm : 1;
   c->cols = cols_per_thread;
@@ -529,8 +535,8 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
     else all_tables = false;
   }
   std::vector<int> nn((size_t)4 * std::max(n_rep, 1));
-  std::vector<long long> off(std::max(n_rep, 1));
-  long long total = 0;
+  std::vector<long long> off(std::max(n_rep, 1)), off_ref(std::max(n_rep, 1));
+  long long total = 0, total_pad = 0;
   for (int r = 0; r < n_rep; r++) {
     const int t = rep_type[r];
     if (t < 0 || t >= n_typ || rep_atom[r] < 0 || rep_atom[r] >= n_atm) return SQB_ERR_ARG;
@@ -538,14 +544,18 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
     nn[4 * r + 1] = nearest_node(rep_xyz[3 * r + 1], c->g.delta);
     nn[4 * r + 2] = nearest_node(rep_xyz[3 * r + 2], c->g.delta);
     nn[4 * r + 3] = t;
-    off[r] = total;
+    off_ref[r] = total;
+    off[r] = total_pad;
     const long long S = 2LL * c->typ_nlocc[t] + 1;
     total += c->typ_nproj[t] * S * S * S;
+    total_pad += c->typ_nproj[t] * S * plane_stride((int)S);
   }
   c->tab_total = total;
+  c->tab_pad_total = total_pad;
   CK(dalloc(&c->d_rep_nn, nn.size()));
   CK(dalloc(&c->d_rep_atom, std::max(n_rep, 1)));
   CK(dalloc(&c->d_rep_off, off.size()));
+  CK(dalloc(&c->d_rep_off_ref, off_ref.size()));
   CK(dalloc(&c->d_rep_xyz, (size_t)3 * std::max(n_rep, 1)));
   CK(dalloc(&c->d_typ_nlocc, std::max(n_typ, 1)));
   CK(dalloc(&c->d_typ_nproj, std::max(n_typ, 1)));
@@ -554,8 +564,10 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
   CK(dalloc(&c->d_typ_size, std::max(n_typ, 1)));
   CK(dalloc(&c->d_typ_tab, std::max(n_typ, 1)));
   CK(dalloc(&c->d_proj_denom, denom.size()));
-  CK(dalloc(&c->d_tab64, (size_t)std::max(total, 1LL)));
-  CK(dalloc(&c->d_tab32, (size_t)std::max(total, 1LL)));
+  CK(dalloc(&c->d_tab64, (size_t)std::max(total_pad, 1LL)));
+  CK(dalloc(&c->d_tab32, (size_t)std::max(total_pad, 1LL)));
+  CK(cudaMemset(c->d_tab64, 0, (size_t)std::max(total_pad, 1LL) * sizeof(double)));
+  CK(cudaMemset(c->d_tab32, 0, (size_t)std::max(total_pad, 1LL) * sizeof(float)));
   CK(dalloc(&c->d_fslots, (size_t)c->nnode * FSLOTS * 4));
   CK(dalloc(&c->d_f, (size_t)3 * std::max(n_atm, 1)));
   CK(cudaMemcpy(c->d_rep_nn, nn.data(), nn.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -564,6 +576,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
     CK(cudaMemcpy(c->d_rep_xyz, rep_xyz, (size_t)3 * n_rep * sizeof(double), cudaMemcpyHostToDevice));
   }
   CK(cudaMemcpy(c->d_rep_off, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_rep_off_ref, off_ref.data(), off_ref.size() * sizeof(long long), cudaMemcpyHostToDevice));
   if (n_typ > 0) {
     CK(cudaMemcpy(c->d_typ_nlocc, c->typ_nlocc.data(), n_typ * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->d_typ_nproj, c->typ_nproj.data(), n_typ * sizeof(int), cudaMemcpyHostToDevice));
@@ -579,6 +592,17 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
     for (int t = 0; t < n_typ; t++)
       CK(cudaMemcpy(c->d_tables + ttab[t], types[t].tables, 19ULL * types[t].size * sizeof(double),
                     cudaMemcpyHostToDevice));
+  }
+  // Size the node kernel's projector-slice stages for the largest per-plane
+  // footprint any window of this block meets.
+  {
+    unsigned *d_fp = reinterpret_cast<unsigned *>(c->d_counter);
+    unsigned fp = 0;
+    CK(launch_plane_footprint(c->n, c->g.nloc, c->g.np, c->g.pnode_s, n_rep, c->d_rep_nn, c->d_typ_nlocc,
+                              c->d_typ_nproj, d_fp, c->stream));
+    CK(cudaMemcpyAsync(&fp, d_fp, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->stage_elems = fp;
   }
   c->have_atoms = true;
   c->have_proj = total == 0;
@@ -613,8 +637,15 @@ int sqb_nonlocal_projectors(sqb_ctx *c, double *udvtm_out) {
   int rc = read_status(c);
   c->stats.ms_projectors = elapsed(c);
   if (rc) return rc;
-  if (udvtm_out && c->tab_total > 0)
-    CK(cudaMemcpy(udvtm_out, c->d_tab64, (size_t)c->tab_total * sizeof(double), cudaMemcpyDeviceToHost));
+  if (udvtm_out && c->tab_total > 0) {
+    rc = ensure_tmp(c, (size_t)c->tab_total * sizeof(double));
+    if (rc) return rc;
+    double *d_ref = reinterpret_cast<double *>(c->d_tmp);
+    CK(launch_repack(c->n_rep, c->d_rep_nn, c->d_typ_nlocc, c->d_typ_nproj, c->d_rep_off_ref, c->d_rep_off,
+                     c->d_tab64, d_ref, 0, c->stream));
+    CK(cudaMemcpyAsync(udvtm_out, d_ref, (size_t)c->tab_total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
   c->have_proj = true;
   c->have_moments = false;
   return SQB_OK;
@@ -625,9 +656,13 @@ int sqb_set_projectors(sqb_ctx *c, const double *udvtm) {
   if (!c->have_atoms) return SQB_ERR_STATE;
   cudaSetDevice(c->device);
   if (c->tab_total > 0) {
-    CK(cudaMemcpyAsync(c->d_tab64, udvtm, (size_t)c->tab_total * sizeof(double), cudaMemcpyHostToDevice,
-                       c->stream));
-    CK(launch_to_float(c->d_tab64, c->d_tab32, c->tab_total, c->stream));
+    int rc = ensure_tmp(c, (size_t)c->tab_total * sizeof(double));
+    if (rc) return rc;
+    double *d_ref = reinterpret_cast<double *>(c->d_tmp);
+    CK(cudaMemcpyAsync(d_ref, udvtm, (size_t)c->tab_total * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(launch_repack(c->n_rep, c->d_rep_nn, c->d_typ_nlocc, c->d_typ_nproj, c->d_rep_off_ref, c->d_rep_off, d_ref,
+                     c->d_tab64, 1, c->stream));
+    CK(launch_to_float(c->d_tab64, c->d_tab32, c->tab_pad_total, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
   c->have_proj = true;

@@ -287,7 +287,7 @@ __global__ void proj_kernel(ProjArgs a) {
       UlJ = UlJ / rad;
     }
     const double u = UlJ * real_sh(xr, yr, zr, rad, l, m) * (VlJ - VlocJ);
-    const long long o = a.rep_off[r] + (long long)q * nnd + ctr;
+    const long long o = a.rep_off[r] + ((long long)q * Sd + ctr / (Sd * Sd)) * plane_stride(Sd) + ctr % (Sd * Sd);
     a.out64[o] = u;
     a.out32[o] = (float)u;
   }
@@ -319,6 +319,20 @@ __global__ void minmax_kernel(const double *lmin, const double *lmax, int n, dou
     }
     out[0] = fmin(a, smin[0]);
     out[1] = fmax(b, smax[0]);
+  }
+}
+
+// Tables between the reference's UdVtm layout [rep][q][Sd^3] and the padded
+// device layout (blockIdx.y = replica).
+__global__ void repack_kernel(const int *rep_nn, const int *typ_nlocc, const int *typ_nproj, const long long *off_ref,
+                              const long long *off_pad, const double *in, double *out, int to_pad) {
+  const int r = blockIdx.y, t = rep_nn[4 * r + 3];
+  const int Sd = 2 * typ_nlocc[t] + 1, sp2 = plane_stride(Sd), S2 = Sd * Sd;
+  const long long cnt = (long long)typ_nproj[t] * Sd * S2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
+    const long long ir = off_ref[r] + i, ip = off_pad[r] + (i / S2) * sp2 + i % S2;
+    if (to_pad) out[ip] = in[ir];
+    else out[ir] = in[ip];
   }
 }
 
@@ -385,6 +399,15 @@ cudaError_t launch_minmax(const double *lmin, const double *lmax, int n, double 
 cudaError_t launch_to_float(const double *in, float *out, long long n, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   to_float_kernel<<<296, 256, 0, s>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_repack(int n_rep, const int *rep_nn, const int *typ_nlocc, const int *typ_nproj,
+                          const long long *off_ref, const long long *off_pad, const double *in, double *out,
+                          int to_pad, cudaStream_t s) {
+  if (n_rep <= 0) return cudaSuccess;
+  dim3 grid(4, n_rep);
+  repack_kernel<<<grid, 256, 0, s>>>(rep_nn, typ_nlocc, typ_nproj, off_ref, off_pad, in, out, to_pad);
   return cudaGetLastError();
 }
 

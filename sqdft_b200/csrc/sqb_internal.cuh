@@ -12,6 +12,15 @@ constexpr int MAXL = 504;        // tridiagonal capacity: 500 Lanczos iterations
 constexpr int LANCZOS_MAX_ITER = 500;
 constexpr int MAXPROJ_TYPE = 16; // (l,m) pairs of one type, l <= 3
 constexpr int FSLOTS = 8;        // replicas whose ball holds one node (force contributions)
+constexpr int MAXN = 64;         // window edge 2*nloc+1
+
+// Projector tables on the device: replica r's table starts at rep_off[r]
+// (a multiple of 4 values) and holds, for each projector q and ball plane z,
+// the Sd x Sd values [y][x] padded to plane_stride(Sd) values, so every
+// (q, z) plane starts 16-byte aligned in FP32 and FP64:
+//   value(q, z, y, x) = tab[rep_off[r] + (q*Sd + z)*plane_stride(Sd) + y*Sd + x].
+// The reference's UdVtm holds the same values without the padding.
+__host__ __device__ __forceinline__ int plane_stride(int Sd) { return (Sd * Sd + 3) & ~3; }
 
 // Device-side status bits (or-ed by the kernels, mapped to SQB_ERR_* on the host).
 enum : int {
@@ -20,6 +29,7 @@ enum : int {
   ST_NONFINITE = 4,
   ST_SPLINE_RANGE = 8,
   ST_FSLOTS = 16,
+  ST_WAIT_LIMIT = 32,  // a bounded wait on an asynchronous copy ran out
 };
 
 // Replica atoms and projector tables as the node kernels read them.
@@ -27,11 +37,11 @@ struct DevAtoms {
   int n_rep;
   const int *rep_nn;        // [n_rep][4]: nearest node x, y, z (global, reference tie rule), type
   const int *rep_atom;      // [n_rep] global atom index
-  const long long *rep_off; // [n_rep] table offset (elements)
+  const long long *rep_off; // [n_rep] padded table offset (elements)
   const int *typ_nlocc;     // [n_typ]
   const int *typ_nproj;     // [n_typ]
   const double *proj_denom; // [n_typ][MAXPROJ_TYPE]
-  const double *tab64;      // concatenated UdVtm, FP64
+  const double *tab64;      // projector tables, padded planes, FP64
   const float *tab32;       // the same in FP32 (mixed path)
 };
 
@@ -58,6 +68,8 @@ struct NodeArgs {
   int *counter;         // work-queue head (zeroed before launch)
   unsigned char *scratch;
   size_t scratch_stride; // bytes per CTA
+  size_t stage_bytes;    // bytes of one projector-slice stage in shared memory (set by the launcher)
+  int row_layout;        // plane-loop layout of the launch: 0 columns, 1 rows (set by the launcher)
   // MODE_SQ outputs, indexed by node id
   double *chi, *zee, *rho_pj, *lmin, *lmax;
   int *lanczos_iters;
@@ -72,10 +84,15 @@ struct NodeArgs {
 };
 
 // Host-side launchers (sqb_node.cu).
-size_t node_kernel_smem(int n, int cols);
 int node_kernel_threads(int n, int cols);
 cudaError_t launch_node_kernel(const NodeArgs &a, int grid, int cols, cudaStream_t s);
 cudaError_t node_kernel_setup(int n);
+// Stage size wanted for a per-plane footprint of `elems` values (the launcher
+// clamps it to what the launch's shared memory leaves).
+size_t node_kernel_stage_bytes(int n, long long elems);
+// Largest per-plane projector-slice footprint over the block's windows -> *d_out.
+cudaError_t launch_plane_footprint(int n, int nloc, const int *np, const int *pnode_s, int n_rep, const int *rep_nn,
+                                   const int *typ_nlocc, const int *typ_nproj, unsigned *d_out, cudaStream_t s);
 
 // Fermi-level and assembly kernels (sqb_fermi.cu).
 struct FermiArgs {
@@ -111,6 +128,10 @@ struct ProjArgs {
 };
 cudaError_t launch_projectors(const ProjArgs &a, cudaStream_t s);
 cudaError_t launch_to_float(const double *in, float *out, long long n, cudaStream_t s);
+// Copy tables between the reference's UdVtm layout and the padded device layout.
+cudaError_t launch_repack(int n_rep, const int *rep_nn, const int *typ_nlocc, const int *typ_nproj,
+                          const long long *off_ref, const long long *off_pad, const double *in, double *out,
+                          int to_pad, cudaStream_t s);
 cudaError_t launch_minmax(const double *lmin, const double *lmax, int n, double *out, cudaStream_t s);
 
 }  // namespace sqb

@@ -57,6 +57,25 @@ def test_spectral_quadrature_fp64(golden, name):
         assert np.abs(f - ref["fnloc"]).max() <= 1e-7
 
 
+@pytest.mark.parametrize("name", ["tiny", "lihs"])
+def test_column_layout_matches_row_layout(golden, name):
+    """The row layout of the plane loop (set_launch(0, -2): a warp per two
+    window rows) gives the same moments and forces as the default column layout."""
+    case, ref = golden(name)
+    with _ctx(case) as ctx:
+        ctx.set_launch(0, -2)
+        rows = ctx.lanczos_moments()
+        f_rows = (ctx.spectral_quadrature(case.scf_iter, case.lambda_f), ctx.forces_nonlocal())[1]
+        ctx.set_launch(0, 0)
+        cols = ctx.lanczos_moments()
+        f_cols = (ctx.spectral_quadrature(case.scf_iter, case.lambda_f), ctx.forces_nonlocal())[1]
+    assert np.array_equal(rows["lanczos_iters"], cols["lanczos_iters"])
+    for k in ("chi", "zee"):
+        assert np.abs(rows[k] - cols[k]).max() <= 1e-12
+    assert np.abs(rows["rho_pj"] - cols["rho_pj"]).max() <= 1e-12 * np.abs(ref["rho_pj"]).max()
+    assert np.abs(f_rows - f_cols).max() <= 1e-10
+
+
 def test_results_al_fermi_level(golden):
     """tests/Al/results_Al:82: first-SCF Fermi level 0.236781162275 Ha."""
     case, ref = golden("al")
