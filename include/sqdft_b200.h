@@ -102,6 +102,7 @@ typedef struct sqb_stats {
   int fermi_iters;
   int max_lanczos_iters;
   int kernel_launches;       /* kernels launched by the last SQ or forces call */
+  double ms_vjp;             /* adjoint node kernel of the last sqb_moments_vjp */
 } sqb_stats;
 
 /* Create a context on CUDA device `device` (cudaSetDevice).  Mirrors the
@@ -165,6 +166,22 @@ int sqb_spectral_quadrature(sqb_ctx *ctx, int scf_iter, double *lambda_f, double
 /* ForcesNonLocal (forces.cpp:318-578) with chi, zee, Ci of the last
  * sqb_spectral_quadrature call (or given ones when not NULL). */
 int sqb_forces_nonlocal(sqb_ctx *ctx, const double *chi, const double *zee, const double *ci, double *forces);
+
+/* Chebyshev moments (sq.cpp:564-655) with given spectral bounds: the node
+ * loop of ClenshawCurtisSpectralQuadrature with chi, zee [nnode] supplied
+ * instead of computed by LanczosAlgorithm.  The bounds become the context's
+ * (sqb_density_energy and sqb_moments_vjp use them).  rho_pj may be NULL. */
+int sqb_moments_at(sqb_ctx *ctx, const double *chi, const double *zee, double *rho_pj);
+
+/* Adjoint of the moments with respect to Veff: given g_mu [nnode][npl+1] =
+ * dL/d rho_pj for a scalar L (rho_pj as sqb_lanczos_moments returns it,
+ * divided by h^3), writes g_veff = dL/dVeff on the Veff block with its halo
+ * (the layout of sqb_set_veff), with the spectral bounds chi, zee of the last
+ * moments held fixed.  Computed by the reverse Chebyshev (Clenshaw) recursion
+ * with checkpoints every 8 recursion vectors.  Contributions of different
+ * nodes to one Veff point are added with atomics, so g_veff varies between
+ * runs at rounding level.  No counterpart in the reference. */
+int sqb_moments_vjp(sqb_ctx *ctx, const double *g_mu, double *g_veff);
 
 /* Size of the fixed device scratch array used by sqb_lanczos_moments_noalloc
  * (held on every GPU that loads the library, until the process exits). */

@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -19,7 +20,7 @@ BUILD = HERE / "_build"
 LIB = BUILD / "libsqdft_b200.so"
 INCLUDE = HERE.parent / "include"
 
-SOURCES = ["sqb_api.cu", "sqb_node.cu", "sqb_fermi.cu"]
+SOURCES = ["sqb_api.cu", "sqb_node.cu", "sqb_node_forces.cu", "sqb_node_vjp.cu", "sqb_fermi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -35,15 +36,20 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> Path:
     deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [INCLUDE / "sqdft_b200.h"]
     if LIB.exists() and not force and all(LIB.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return LIB
-    objs = []
+    cmds, objs = [], []
     for src in SOURCES:
         obj = BUILD / (Path(src).stem + ".o")
         cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                f"-I{INCLUDE}", "-c", str(CSRC / src), "-o", str(obj)]
         if verbose_ptxas:
             cmd.insert(-4, "-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=len(cmds)) as pool:
+        for r in pool.map(lambda c: subprocess.run(c, check=False), cmds):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
     tmp.replace(LIB)

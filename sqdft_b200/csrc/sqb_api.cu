@@ -48,6 +48,8 @@ struct sqb_ctx {
   long long tab_total = 0;      // values of the reference's UdVtm
   long long tab_pad_total = 0;  // values of the padded device tables
   long long *d_rep_off_ref = nullptr;
+  double *d_vjp = nullptr;  // adjoint: per-CTA scratch, dL/dmu, dL/dVeff
+  size_t vjp_bytes = 0;
   long long stage_elems = 0;  // largest per-plane projector-slice footprint (values)
   bool have_atoms = false, have_proj = false;
 
@@ -446,7 +448,7 @@ int sqb_destroy(sqb_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void *ptrs[] = {c->d_veff64, c->d_veff32, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
                   c->d_typ_nlocc, c->d_typ_nproj, c->d_typ_lmax, c->d_typ_lloc, c->d_typ_size, c->d_proj_denom,
-                  c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_tab64, c->d_tab32, c->d_scratch, c->d_counter, c->d_nodes,
+                  c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_tab64, c->d_tab32, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
                   c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
                   c->d_f, c->d_tmp};
@@ -820,6 +822,76 @@ int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *
   if (rc) return rc;
   *lambda_f = lam;
   return sqb_density_energy(c, lam, rho, ci, ebs, eent);
+}
+
+int sqb_moments_at(sqb_ctx *c, const double *chi, const double *zee, double *rho_pj) {
+  if (!c || !chi || !zee) return SQB_ERR_ARG;
+  if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
+  const size_t N = c->nnode, K = c->g.npl + 1;
+  for (size_t i = 0; i < N; i++)
+    if (!std::isfinite(chi[i]) || !(zee[i] > 0.0) || !std::isfinite(zee[i])) return SQB_ERR_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaMemcpy(c->d_chi, chi, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_zee, zee, N * sizeof(double), cudaMemcpyHostToDevice));
+  NodeArgs a;
+  fill_node_args(c, a);
+  a.mode = MODE_MOMENTS;
+  a.chi_in = c->d_chi;
+  a.zee_in = c->d_zee;
+  a.rho_pj = c->d_rho_pj;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = run_nodes(c, a, c->d_nodes, c->nnode);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  rc = read_status(c);
+  c->stats.ms_lanczos_moments = elapsed(c);
+  if (rc) return rc;
+  c->have_moments = true;
+  c->have_ci = false;
+  if (rho_pj) CK(cudaMemcpy(rho_pj, c->d_rho_pj, N * K * sizeof(double), cudaMemcpyDeviceToHost));
+  return SQB_OK;
+}
+
+int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff) {
+  if (!c || !g_mu || !g_veff) return SQB_ERR_ARG;
+  if (!c->have_moments) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  const size_t N = c->nnode, K = c->g.npl + 1;
+  const size_t nw = (size_t)c->n * c->n * c->n;
+  const size_t ext = (size_t)c->ex * c->ey * c->ez;
+  const int nseg = (c->g.npl + VJP_K - 1) / VJP_K;
+  const size_t per = ((size_t)(2 * nseg + VJP_K + 4) * nw + (size_t)nseg * MAXP + 31) & ~size_t(31);  // doubles
+  int grid = c->sms * (c->ctas_per_sm > 0 ? c->ctas_per_sm : 1);
+  if ((size_t)grid > N) grid = (int)N;
+  const size_t need = (per * grid + N * K + ext) * sizeof(double);
+  if (c->vjp_bytes < need) {
+    if (c->d_vjp) cudaFree(c->d_vjp);
+    c->d_vjp = nullptr;
+    c->vjp_bytes = 0;
+    CK(cudaMalloc((void **)&c->d_vjp, need));
+    c->vjp_bytes = need;
+  }
+  double *d_scr = c->d_vjp, *d_g = d_scr + per * grid, *d_out = d_g + N * K;
+  CK(cudaMemcpyAsync(d_g, g_mu, N * K * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(d_out, 0, ext * sizeof(double), c->stream));
+  NodeArgs a;
+  fill_node_args(c, a);
+  a.mode = MODE_VJP;
+  a.chi_in = c->d_chi;
+  a.zee_in = c->d_zee;
+  a.gmu = d_g;
+  a.vjp = d_scr;
+  a.vjp_stride = per;
+  a.g_veff = d_out;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = run_nodes(c, a, c->d_nodes, c->nnode);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  rc = read_status(c);
+  c->stats.ms_vjp = elapsed(c);
+  if (rc) return rc;
+  CK(cudaMemcpy(g_veff, d_out, ext * sizeof(double), cudaMemcpyDeviceToHost));
+  return SQB_OK;
 }
 
 int sqb_forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const double *ci, double *forces) {

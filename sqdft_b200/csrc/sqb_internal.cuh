@@ -45,7 +45,8 @@ struct DevAtoms {
   const float *tab32;       // the same in FP32 (mixed path)
 };
 
-enum NodeMode : int { MODE_SQ = 0, MODE_FORCES = 1, MODE_APPLY = 2 };
+enum NodeMode : int { MODE_SQ = 0, MODE_FORCES = 1, MODE_APPLY = 2, MODE_MOMENTS = 3, MODE_VJP = 4 };
+constexpr int VJP_K = 8;  // adjoint: checkpoint every VJP_K recursion vectors
 
 struct NodeArgs {
   int mode;
@@ -79,6 +80,12 @@ struct NodeArgs {
   // MODE_APPLY
   const double *apply_in;
   double *apply_out;
+  // MODE_VJP: dL/dmu per node [nnode][npl+1], per-CTA scratch, dL/dVeff on the
+  // Veff block with halo (accumulated with atomics)
+  const double *gmu;
+  double *vjp;
+  size_t vjp_stride;  // doubles per CTA
+  double *g_veff;
   int *status;
   unsigned long long *proj_points; // algorithmic projector-ball points touched
 };
@@ -86,6 +93,11 @@ struct NodeArgs {
 // Host-side launchers (sqb_node.cu).
 int node_kernel_threads(int n, int cols);
 cudaError_t launch_node_kernel(const NodeArgs &a, int grid, int cols, cudaStream_t s);
+// Kernel groups compiled in their own translation units (sqb_node_forces.cu, sqb_node_vjp.cu).
+cudaError_t setup_node_forces(int n);
+cudaError_t launch_node_forces(const NodeArgs &a, int grid, int cols, cudaStream_t s);
+cudaError_t setup_node_vjp(int n);
+cudaError_t launch_node_vjp(const NodeArgs &a, int grid, int cols, cudaStream_t s);
 cudaError_t node_kernel_setup(int n);
 // Stage size wanted for a per-plane footprint of `elems` values (the launcher
 // clamps it to what the launch's shared memory leaves).

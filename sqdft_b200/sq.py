@@ -35,7 +35,7 @@ EXPORTS = [
     "sqb_set_atoms", "sqb_nonlocal_projectors", "sqb_set_projectors", "sqb_hsub_times_vec",
     "sqb_lanczos_moments", "sqb_ne_constraint", "sqb_fermi_level", "sqb_density_energy",
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
-    "sqb_lanczos_moments_noalloc",
+    "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp",
 ]
 
 
@@ -56,7 +56,8 @@ class SqbStats(C.Structure):
                 ("ms_forces", C.c_double), ("ms_projectors", C.c_double), ("matvecs", C.c_longlong),
                 ("lanczos_iters", C.c_longlong), ("window_points", C.c_longlong), ("proj_points", C.c_longlong),
                 ("proj_points_cheb", C.c_longlong),
-                ("fermi_iters", C.c_int), ("max_lanczos_iters", C.c_int), ("kernel_launches", C.c_int)]
+                ("fermi_iters", C.c_int), ("max_lanczos_iters", C.c_int), ("kernel_launches", C.c_int),
+                ("ms_vjp", C.c_double)]
 
 
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, _dp, C.c_int, C.c_int, C.c_void_p)
@@ -97,6 +98,8 @@ def library() -> C.CDLL:
         lib.sqb_forces_nonlocal.argtypes = [P, _dp, _dp, _dp, _dp]
         lib.sqb_get_stats.argtypes = [P, C.POINTER(SqbStats), C.c_size_t]
         lib.sqb_lanczos_moments_noalloc.argtypes = [P, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.sqb_moments_at.argtypes = [P, _dp, _dp, _dp]
+        lib.sqb_moments_vjp.argtypes = [P, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
         lib.sqb_version.restype = C.c_char_p
@@ -185,8 +188,15 @@ class Context:
         self._cb = ALLREDUCE_FN(cb)
         _check(self.lib.sqb_set_allreduce(self.ptr, self._cb, None), "sqb_set_allreduce")
 
+    def _veff_ext_shape(self) -> tuple[int, int, int]:
+        """Veff block with its halo: [np_z + 2nloc][np_y + 2nloc][np_x + 2nloc]."""
+        c, nl = self.case, self.case.nloc
+        return (c.np_[2] + 2 * nl, c.np_[1] + 2 * nl, c.np_[0] + 2 * nl)
+
     def set_veff(self, veff_ext: np.ndarray):
         v = np.ascontiguousarray(veff_ext, np.float64)
+        if v.size != int(np.prod(self._veff_ext_shape())):
+            raise ValueError(f"Veff with halo must have shape {self._veff_ext_shape()}, got {v.shape}")
         _check(self.lib.sqb_set_veff(self.ptr, _d(v)), "sqb_set_veff")
 
     def set_atoms(self, case: Case):
@@ -237,6 +247,24 @@ class Context:
                                             _i(r["lanczos_iters"]), _d(r["lmin"]), _d(r["lmax"])),
                "sqb_lanczos_moments")
         return r
+
+    def moments_at(self, chi: np.ndarray, zee: np.ndarray) -> np.ndarray:
+        """Chebyshev moments rho_pj [nnode][npl+1] with the given spectral bounds."""
+        c = self.case
+        chi = np.ascontiguousarray(chi, np.float64)
+        zee = np.ascontiguousarray(zee, np.float64)
+        rho_pj = np.zeros((c.n_nodes, c.npl + 1))
+        _check(self.lib.sqb_moments_at(self.ptr, _d(chi), _d(zee), _d(rho_pj)), "sqb_moments_at")
+        return rho_pj
+
+    def moments_vjp(self, g_mu: np.ndarray) -> np.ndarray:
+        """dL/dVeff on the Veff block with halo for dL/drho_pj = g_mu (bounds of the
+        last moments held fixed)."""
+        c = self.case
+        g = np.ascontiguousarray(g_mu, np.float64).reshape(c.n_nodes, c.npl + 1)
+        out = np.zeros(self._veff_ext_shape())
+        _check(self.lib.sqb_moments_vjp(self.ptr, _d(g), _d(out)), "sqb_moments_vjp")
+        return out
 
     def ne_constraint(self, lam: float) -> float:
         v = C.c_double()
