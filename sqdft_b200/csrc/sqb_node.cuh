@@ -397,15 +397,15 @@ __device__ void rotate_proj(NodeShared &S, double scale) {
   __syncthreads();
 }
 
-// PK_LZF input at window index g: the next (unnormalised) Lanczos vector
+// PK_LZF input at window index g from its loaded operands y = Y[g],
+// w1 = W1[g], w2 = W2[g]: the next (unnormalised) Lanczos vector
 // W = s1 (Y - ca W1) - cb W2, i.e. u - a v_k - b v_k-1 with u = s1 Y,
 // v_k = s1 W1, v_k-1 = s2 W2 and cb = b s2 (LanczosAlgorithm, sq.cpp:1032-1036);
-// stored in wout, in place of W2.
+// stored in wout, in place of W2.  The operands are loaded one plane before
+// they are combined, so the loads' latency overlaps a plane of work.
 template <typename T>
-__device__ __forceinline__ T form_w(const PassIO<T> &io, size_t g) {
-  T f;
-  if (io.konst) f = (T)io.sin;
-  else f = (T)(io.s1 * ((double)io.vin[g] - io.ca * (double)io.p1[g]) - io.cb * (double)io.p2[g]);
+__device__ __forceinline__ T form_w(const PassIO<T> &io, size_t g, T y, T w1, T w2) {
+  const T f = io.konst ? (T)io.sin : (T)(io.s1 * ((double)y - io.ca * (double)w1) - io.cb * (double)w2);
   io.wout[g] = f;
   return f;
 }
@@ -452,12 +452,24 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
   auto ld_in = [&](int c, int z) -> T {
     if (!ok[c] || z >= n) return T(0);
     if constexpr (PK == PK_DOTS || PK == PK_APPLY) return (T)io.din[(size_t)z * n2 + col[c]];
-    else if constexpr (PK == PK_LZF) return form_w<T>(io, (size_t)z * n2 + col[c]);
     else return io.vin[(size_t)z * n2 + col[c]] * sin;
   };
 
   T win[C][2 * FDN + 1];
   T pf[C];
+  T rw1[C], rw2[C];  // PK_LZF: W1, W2 of the prefetched plane (pf holds its Y)
+  auto lzf_load = [&](int c, int z) {
+    if (ok[c] && z < n && !io.konst) {
+      const size_t g = (size_t)z * n2 + col[c];
+      pf[c] = io.vin[g];
+      rw1[c] = io.p1[g];
+      rw2[c] = io.p2[g];
+    }
+  };
+  auto lzf_form = [&](int c, int z) -> T {
+    if (!ok[c] || z >= n) return T(0);
+    return form_w<T>(io, (size_t)z * n2 + col[c], pf[c], rw1[c], rw2[c]);
+  };
   T q_ve[C], q_p1[C], q_p2[C];
   double q_d[C];
   auto ld_point = [&](int c, int z) {
@@ -472,7 +484,35 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
   };
 #pragma unroll
   for (int c = 0; c < C; c++) {
-    if constexpr (STENCIL) {
+    if constexpr (PK == PK_LZF) {
+      // planes 0..FDN enter the window: their operands are loaded four planes
+      // at a time before any is combined (the stores of W would otherwise
+      // order every load after the previous plane's store)
+#pragma unroll
+      for (int s = 0; s < FDN; s++) win[c][s] = T(0);
+#pragma unroll
+      for (int z0 = 0; z0 <= FDN; z0 += 4) {
+        T ty[4], t1[4], t2[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int z = z0 + q;
+          ty[q] = t1[q] = t2[q] = T(0);
+          if (z <= FDN && ok[c] && z < n && !io.konst) {
+            const size_t g = (size_t)z * n2 + col[c];
+            ty[q] = io.vin[g];
+            t1[q] = io.p1[g];
+            t2[q] = io.p2[g];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int z = z0 + q;
+          if (z <= FDN)
+            win[c][FDN + z] = (ok[c] && z < n) ? form_w<T>(io, (size_t)z * n2 + col[c], ty[q], t1[q], t2[q]) : T(0);
+        }
+      }
+      lzf_load(c, FDN + 1);
+    } else if constexpr (STENCIL) {
 #pragma unroll
       for (int s = 0; s <= 2 * FDN; s++) win[c][s] = s < FDN ? T(0) : ld_in(c, s - FDN);
       pf[c] = ld_in(c, FDN + 1);
@@ -617,7 +657,12 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
     // advance the register windows and prefetch the next plane's operands
 #pragma unroll
     for (int c = 0; c < C; c++) {
-      if constexpr (STENCIL) {
+      if constexpr (PK == PK_LZF) {
+#pragma unroll
+        for (int s = 0; s < 2 * FDN; s++) win[c][s] = win[c][s + 1];
+        win[c][2 * FDN] = lzf_form(c, z + FDN + 1);
+        lzf_load(c, z + FDN + 2);
+      } else if constexpr (STENCIL) {
 #pragma unroll
         for (int s = 0; s < 2 * FDN; s++) win[c][s] = win[c][s + 1];
         win[c][2 * FDN] = pf[c];
@@ -685,11 +730,23 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
   auto ld_in = [&](int j, int z) -> T {
     if (!ok[j] || z >= n) return T(0);
     if constexpr (PK == PK_DOTS || PK == PK_APPLY) return (T)io.din[(size_t)z * n2 + col[j]];
-    else if constexpr (PK == PK_LZF) return form_w<T>(io, (size_t)z * n2 + col[j]);
     else return io.vin[(size_t)z * n2 + col[j]] * sin;
   };
   T win[RY][2 * FDN + 1];
   T pf[RY], q_ve[RY], q_p1[RY], q_p2[RY];
+  T rw1[RY], rw2[RY];  // PK_LZF: W1, W2 of the prefetched plane (pf holds its Y)
+  auto lzf_load = [&](int j, int z) {
+    if (ok[j] && z < n && !io.konst) {
+      const size_t g = (size_t)z * n2 + col[j];
+      pf[j] = io.vin[g];
+      rw1[j] = io.p1[g];
+      rw2[j] = io.p2[g];
+    }
+  };
+  auto lzf_form = [&](int j, int z) -> T {
+    if (!ok[j] || z >= n) return T(0);
+    return form_w<T>(io, (size_t)z * n2 + col[j], pf[j], rw1[j], rw2[j]);
+  };
   double q_d[RY];
   auto ld_point = [&](int j, int z) {
     if (!ok[j] || z >= n) return;
@@ -702,7 +759,32 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
   };
 #pragma unroll
   for (int j = 0; j < RY; j++) {
-    if constexpr (STENCIL) {
+    if constexpr (PK == PK_LZF) {
+#pragma unroll
+      for (int s = 0; s < FDN; s++) win[j][s] = T(0);
+#pragma unroll
+      for (int z0 = 0; z0 <= FDN; z0 += 4) {
+        T ty[4], t1[4], t2[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int z = z0 + q;
+          ty[q] = t1[q] = t2[q] = T(0);
+          if (z <= FDN && ok[j] && z < n && !io.konst) {
+            const size_t g = (size_t)z * n2 + col[j];
+            ty[q] = io.vin[g];
+            t1[q] = io.p1[g];
+            t2[q] = io.p2[g];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int z = z0 + q;
+          if (z <= FDN)
+            win[j][FDN + z] = (ok[j] && z < n) ? form_w<T>(io, (size_t)z * n2 + col[j], ty[q], t1[q], t2[q]) : T(0);
+        }
+      }
+      lzf_load(j, FDN + 1);
+    } else if constexpr (STENCIL) {
 #pragma unroll
       for (int s = 0; s <= 2 * FDN; s++) win[j][s] = s < FDN ? T(0) : ld_in(j, s - FDN);
       pf[j] = ld_in(j, FDN + 1);
@@ -901,7 +983,12 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
     }
 #pragma unroll
     for (int j = 0; j < RY; j++) {
-      if constexpr (STENCIL) {
+      if constexpr (PK == PK_LZF) {
+#pragma unroll
+        for (int s = 0; s < 2 * FDN; s++) win[j][s] = win[j][s + 1];
+        win[j][2 * FDN] = lzf_form(j, z + FDN + 1);
+        lzf_load(j, z + FDN + 2);
+      } else if constexpr (STENCIL) {
 #pragma unroll
         for (int s = 0; s < 2 * FDN; s++) win[j][s] = win[j][s + 1];
         win[j][2 * FDN] = pf[j];
