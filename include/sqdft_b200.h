@@ -117,6 +117,27 @@ int sqb_set_allreduce(sqb_ctx *ctx, sqb_allreduce_fn fn, void *user);
  * row layout (a warp per two window rows, windows up to 32 wide). */
 int sqb_set_launch(sqb_ctx *ctx, int ctas_per_sm, int cols_per_thread);
 
+/* CUDA-graph replay of the node-kernel sequence of sqb_lanczos_moments (and
+ * so of the SQ step): work-queue and status resets, the persistent Lanczos +
+ * Chebyshev launch and the bound min/max, captured on the first call after
+ * a plain run has allocated their buffers and replayed afterwards; dropped
+ * when atoms, launch layout or precision change.  The Fermi-level solve stays
+ * host-driven (one launch per Brent or Newton trial, as the reference's
+ * control flow).  on: 1 = use, 0 = plain launches (default). */
+int sqb_set_graph(sqb_ctx *ctx, int on);
+
+/* Autotuner of the node kernel's plane-loop layout: times the Lanczos +
+ * moments kernel on `sample` evenly spaced nodes (0 = two per SM) with every
+ * layout the window allows -- one or two window columns per thread, and the
+ * row layout for windows up to 32 wide -- and keeps the fastest for the
+ * context, as sqb_set_launch(ctx, 0, layout) would.  *chosen receives the
+ * layout; ms_out (3 doubles, or NULL) the sample times for 1, 2 and -2
+ * (negative where a layout does not apply).  The sample runs overwrite part
+ * of the per-node outputs, so run sqb_lanczos_moments (or the SQ step)
+ * afterwards.  Results do not depend on the layout.  No counterpart in the
+ * reference. */
+int sqb_autotune(sqb_ctx *ctx, int sample, int *chosen, double *ms_out);
+
 /* Veff on the block with its Rcut halo: the state of DS_SQ::Veff after the
  * halo exchange of sq.cpp:400-492. */
 int sqb_set_veff(sqb_ctx *ctx, const double *veff_ext);

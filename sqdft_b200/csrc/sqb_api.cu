@@ -26,6 +26,9 @@ struct sqb_ctx {
   cudaStream_t stream = nullptr;
   int precision = SQB_FP64;
   int cols = 0, ctas_per_sm = 1;
+  int use_graph = 0;                       // replay the node-kernel sequence from a CUDA graph
+  cudaGraphExec_t sq_graph = nullptr;      // captured Lanczos+moments sequence (node kernel, min/max)
+  int sq_graph_warm = 0;                   // a plain run has allocated what the sequence uses
   int n = 0, nnode = 0, ex = 0, ey = 0, ez = 0;
   double h3 = 0.0;
   sqb_allreduce_fn allreduce = nullptr;
@@ -350,6 +353,13 @@ float elapsed(sqb_ctx *c) {
   return ms;
 }
 
+// Drop the captured SQ sequence (its kernel arguments may have changed).
+void drop_graph(sqb_ctx *c) {
+  if (c->sq_graph) cudaGraphExecDestroy(c->sq_graph);
+  c->sq_graph = nullptr;
+  c->sq_graph_warm = 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -454,6 +464,7 @@ int sqb_destroy(sqb_ctx *c) {
                   c->d_f, c->d_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  drop_graph(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -464,6 +475,7 @@ int sqb_destroy(sqb_ctx *c) {
 int sqb_set_precision(sqb_ctx *c, int precision) {
   if (!c || (precision != SQB_FP64 && precision != SQB_FP32_MIXED)) return SQB_ERR_ARG;
   c->precision = precision;
+  drop_graph(c);
   return SQB_OK;
 }
 
@@ -482,6 +494,7 @@ int sqb_set_launch(sqb_ctx *c, int ctas_per_sm, int cols_per_thread) {
   if (cols_per_thread > 0 && node_kernel_threads(c->n, cols_per_thread) > 1024) return SQB_ERR_UNSUPPORTED;
   c->ctas_per_sm = ctas_per_sm > 0 ? ctas_per_sm : 1;
   c->cols = cols_per_thread;
+  drop_graph(c);
   return SQB_OK;
 }
 
@@ -607,6 +620,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
     c->stage_elems = fp;
   }
   c->have_atoms = true;
+  drop_graph(c);
   c->have_proj = total == 0;
   c->have_moments = false;
   return SQB_OK;
@@ -714,10 +728,30 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   a.lmax = c->d_lmax;
   a.lanczos_iters = c->d_iters;
   c->stats.kernel_launches = 0;
+  int rc = SQB_OK;
+  if (c->use_graph && c->sq_graph_warm && !c->sq_graph) {
+    // capture the sequence once its buffers exist (a plain run allocated them)
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    rc = run_nodes(c, a, c->d_nodes, c->nnode);
+    if (!rc && launch_minmax(c->d_lmin, c->d_lmax, c->nnode, c->d_result, c->stream) != cudaSuccess) rc = SQB_ERR_CUDA;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (!rc && e == cudaSuccess && cudaGraphInstantiate(&c->sq_graph, g, 0) != cudaSuccess) c->sq_graph = nullptr;
+    if (g) cudaGraphDestroy(g);
+    if (rc || e != cudaSuccess || !c->sq_graph) {
+      c->use_graph = 0;  // fall back to plain launches
+      cudaGetLastError();
+    }
+  }
   CK(cudaEventRecord(c->ev0, c->stream));
-  int rc = run_nodes(c, a, c->d_nodes, c->nnode);
-  if (rc) return rc;
-  CK(launch_minmax(c->d_lmin, c->d_lmax, c->nnode, c->d_result, c->stream));
+  if (c->use_graph && c->sq_graph) {
+    CK(cudaGraphLaunch(c->sq_graph, c->stream));
+  } else {
+    rc = run_nodes(c, a, c->d_nodes, c->nnode);
+    if (rc) return rc;
+    CK(launch_minmax(c->d_lmin, c->d_lmax, c->nnode, c->d_result, c->stream));
+    c->sq_graph_warm = 1;
+  }
   CK(cudaEventRecord(c->ev1, c->stream));
   c->stats.kernel_launches += 2;
   rc = read_status(c);
@@ -822,6 +856,74 @@ int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *
   if (rc) return rc;
   *lambda_f = lam;
   return sqb_density_energy(c, lam, rho, ci, ebs, eent);
+}
+
+int sqb_set_graph(sqb_ctx *c, int on) {
+  if (!c || (on != 0 && on != 1)) return SQB_ERR_ARG;
+  c->use_graph = on;
+  drop_graph(c);
+  return SQB_OK;
+}
+
+int sqb_autotune(sqb_ctx *c, int sample, int *chosen, double *ms_out) {
+  if (!c || sample < 0) return SQB_ERR_ARG;
+  if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  const int N = c->nnode;
+  int count = sample > 0 ? sample : 2 * c->sms;
+  if (count > N) count = N;
+  std::vector<int> list(count);
+  for (int i = 0; i < count; i++) list[i] = (int)((long long)i * N / count);  // evenly spaced nodes
+  int rc = ensure_tmp(c, (size_t)count * sizeof(int));
+  if (rc) return rc;
+  int *d_list = reinterpret_cast<int *>(c->d_tmp);
+  CK(cudaMemcpy(d_list, list.data(), (size_t)count * sizeof(int), cudaMemcpyHostToDevice));
+  const int cands[3] = {1, 2, -2};
+  double ms[3] = {-1.0, -1.0, -1.0};
+  const int keep = c->cols;
+  int best = -1;
+  for (int k = 0; k < 3; k++) {
+    const int cols = cands[k];
+    if (cols == -2 && c->n > 32) continue;
+    if (node_kernel_threads(c->n, cols) > 1024) continue;
+    c->cols = cols;
+    NodeArgs a;
+    fill_node_args(c, a);
+    a.mode = MODE_SQ;
+    a.chi = c->d_chi;
+    a.zee = c->d_zee;
+    a.rho_pj = c->d_rho_pj;
+    a.lmin = c->d_lmin;
+    a.lmax = c->d_lmax;
+    a.lanczos_iters = c->d_iters;
+    float t = 0.f;
+    for (int rep = 0; rep < 2; rep++) {  // the first launch of a variant is a warm-up
+      CK(cudaEventRecord(c->ev0, c->stream));
+      rc = run_nodes(c, a, d_list, count);
+      if (rc) {
+        c->cols = keep;
+        return rc;
+      }
+      CK(cudaEventRecord(c->ev1, c->stream));
+      rc = read_status(c);
+      if (rc) {
+        c->cols = keep;
+        return rc;
+      }
+      t = elapsed(c);
+    }
+    ms[k] = t;
+    if (best < 0 || ms[k] < ms[best]) best = k;
+  }
+  c->cols = best >= 0 ? cands[best] : keep;
+  drop_graph(c);
+  // the sample runs overwrote part of the per-node outputs
+  c->have_moments = false;
+  c->have_ci = false;
+  if (chosen) *chosen = c->cols;
+  if (ms_out)
+    for (int k = 0; k < 3; k++) ms_out[k] = ms[k];
+  return SQB_OK;
 }
 
 int sqb_moments_at(sqb_ctx *c, const double *chi, const double *zee, double *rho_pj) {

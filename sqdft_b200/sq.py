@@ -35,7 +35,8 @@ EXPORTS = [
     "sqb_set_atoms", "sqb_nonlocal_projectors", "sqb_set_projectors", "sqb_hsub_times_vec",
     "sqb_lanczos_moments", "sqb_ne_constraint", "sqb_fermi_level", "sqb_density_energy",
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
-    "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp",
+    "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
+    "sqb_set_graph",
 ]
 
 
@@ -99,6 +100,8 @@ def library() -> C.CDLL:
         lib.sqb_get_stats.argtypes = [P, C.POINTER(SqbStats), C.c_size_t]
         lib.sqb_lanczos_moments_noalloc.argtypes = [P, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.sqb_moments_at.argtypes = [P, _dp, _dp, _dp]
+        lib.sqb_autotune.argtypes = [P, C.c_int, _ip, _dp]
+        lib.sqb_set_graph.argtypes = [P, C.c_int]
         lib.sqb_moments_vjp.argtypes = [P, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
@@ -173,6 +176,17 @@ class Context:
 
     def set_launch(self, ctas_per_sm: int = 0, cols_per_thread: int = 0):
         _check(self.lib.sqb_set_launch(self.ptr, ctas_per_sm, cols_per_thread), "sqb_set_launch")
+
+    def set_graph(self, on: bool = True):
+        _check(self.lib.sqb_set_graph(self.ptr, int(bool(on))), "sqb_set_graph")
+
+    def autotune(self, sample: int = 0):
+        """Pick the node kernel's layout by timing a node sample; returns the
+        chosen layout and {layout: ms} for the layouts that apply."""
+        chosen = C.c_int()
+        ms = np.zeros(3)
+        _check(self.lib.sqb_autotune(self.ptr, sample, C.byref(chosen), _d(ms)), "sqb_autotune")
+        return chosen.value, {k: v for k, v in zip((1, 2, -2), ms) if v >= 0}
 
     def set_allreduce(self, fn):
         """fn(values: np.ndarray, op: int) -> None, reducing in place across ranks."""

@@ -138,3 +138,39 @@ def test_newton_fermi_and_warm_bracket(golden):
         ctx.lanczos_moments()
         lam, _ = ctx.fermi_level(1, 0.0)
         assert abs(lam - lam_n) <= 1e-10
+
+
+def test_autotune_picks_a_layout_and_keeps_results(golden):
+    """sqb_autotune times the layouts on a node sample, keeps the fastest; the
+    SQ results afterwards equal the default layout's."""
+    case, _ = golden("mid")
+    with _ctx(case) as ctx:
+        base = ctx.lanczos_moments()
+        chosen, times = ctx.autotune()
+        assert chosen in times and times[chosen] == min(times.values())
+        assert set(times) == {1, 2, -2}  # 15^3 windows: every layout applies
+        after = ctx.lanczos_moments()
+    assert np.array_equal(base["lanczos_iters"], after["lanczos_iters"])
+    assert np.abs(base["rho_pj"] - after["rho_pj"]).max() <= 1e-12 * np.abs(base["rho_pj"]).max()
+
+
+def test_graph_replay_matches_plain_launches(golden):
+    """The node-kernel sequence replayed from a CUDA graph (captured on the
+    second call, replayed on the third) gives the plain launch's results;
+    changing Veff between replays is seen (the graph reads device buffers)."""
+    case, _ = golden("tiny")
+    with _ctx(case) as ctx:
+        plain = ctx.lanczos_moments()
+        ctx.set_graph(True)
+        first = ctx.lanczos_moments()   # plain run, then capture on the next call
+        second = ctx.lanczos_moments()  # captured and launched
+        third = ctx.lanczos_moments()   # replay
+        ctx.set_veff(case.veff * 1.01)
+        moved = ctx.lanczos_moments()   # replay with the new Veff
+        ctx.set_graph(False)
+        moved_plain = ctx.lanczos_moments()
+    for r in (first, second, third):
+        assert np.array_equal(r["lanczos_iters"], plain["lanczos_iters"])
+        assert np.array_equal(r["rho_pj"], plain["rho_pj"])
+    assert np.array_equal(moved["rho_pj"], moved_plain["rho_pj"])
+    assert not np.array_equal(moved["rho_pj"], plain["rho_pj"])
