@@ -194,15 +194,19 @@ int sqb_forces_nonlocal(sqb_ctx *ctx, const double *chi, const double *zee, cons
  * (sqb_density_energy and sqb_moments_vjp use them).  rho_pj may be NULL. */
 int sqb_moments_at(sqb_ctx *ctx, const double *chi, const double *zee, double *rho_pj);
 
-/* Adjoint of the moments with respect to Veff: given g_mu [nnode][npl+1] =
- * dL/d rho_pj for a scalar L (rho_pj as sqb_lanczos_moments returns it,
- * divided by h^3), writes g_veff = dL/dVeff on the Veff block with its halo
- * (the layout of sqb_set_veff), with the spectral bounds chi, zee of the last
- * moments held fixed.  Computed by the reverse Chebyshev (Clenshaw) recursion
- * with checkpoints every 8 recursion vectors.  Contributions of different
- * nodes to one Veff point are added with atomics, so g_veff varies between
- * runs at rounding level.  No counterpart in the reference. */
-int sqb_moments_vjp(sqb_ctx *ctx, const double *g_mu, double *g_veff);
+/* Adjoint of the moments: given g_mu [nnode][npl+1] = dL/d rho_pj for a
+ * scalar L (rho_pj as sqb_lanczos_moments returns it, divided by h^3), writes
+ * g_veff = dL/dVeff on the Veff block with its halo (the layout of
+ * sqb_set_veff) and, when g_atoms is not NULL, g_atoms = dL/dR [n_atm][3]
+ * (type-major, the layout of sqb_forces_nonlocal) through the projector
+ * tables, with the spectral bounds chi, zee of the last moments held fixed.
+ * Computed by the reverse Chebyshev (Clenshaw) recursion with checkpoints
+ * every 8 recursion vectors; the projector derivatives dchi/dR are central
+ * differences (step 1e-4 bohr) of the projector tables.  Contributions of
+ * different nodes to one Veff point or atom are added with atomics, so the
+ * outputs vary between runs at rounding level.  No counterpart in the
+ * reference. */
+int sqb_moments_vjp(sqb_ctx *ctx, const double *g_mu, double *g_veff, double *g_atoms);
 
 /* Size of the fixed device scratch array used by sqb_lanczos_moments_noalloc
  * (held on every GPU that loads the library, until the process exits). */

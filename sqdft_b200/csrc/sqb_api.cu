@@ -53,6 +53,11 @@ struct sqb_ctx {
   long long *d_rep_off_ref = nullptr;
   double *d_vjp = nullptr;  // adjoint: per-CTA scratch, dL/dmu, dL/dVeff
   size_t vjp_bytes = 0;
+  double *d_vjp_at = nullptr;  // adjoint with atom gradients: per-CTA scratch, dL/dR
+  size_t vjp_at_bytes = 0;
+  double *d_dtab = nullptr;    // dchi/dR_alpha tables, 3 x tab_pad_total
+  bool have_dtab = false;
+  std::vector<double> h_rep_xyz;  // replica positions (for the derivative tables)
   long long stage_elems = 0;  // largest per-plane projector-slice footprint (values)
   bool have_atoms = false, have_proj = false;
 
@@ -458,7 +463,7 @@ int sqb_destroy(sqb_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void *ptrs[] = {c->d_veff64, c->d_veff32, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
                   c->d_typ_nlocc, c->d_typ_nproj, c->d_typ_lmax, c->d_typ_lloc, c->d_typ_size, c->d_proj_denom,
-                  c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_tab64, c->d_tab32, c->d_scratch, c->d_counter, c->d_nodes,
+                  c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_tab32, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
                   c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
                   c->d_f, c->d_tmp};
@@ -589,6 +594,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
   if (n_rep > 0) {
     CK(cudaMemcpy(c->d_rep_atom, rep_atom, n_rep * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->d_rep_xyz, rep_xyz, (size_t)3 * n_rep * sizeof(double), cudaMemcpyHostToDevice));
+    c->h_rep_xyz.assign(rep_xyz, rep_xyz + (size_t)3 * n_rep);
   }
   CK(cudaMemcpy(c->d_rep_off, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_rep_off_ref, off_ref.data(), off_ref.size() * sizeof(long long), cudaMemcpyHostToDevice));
@@ -620,6 +626,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
     c->stage_elems = fp;
   }
   c->have_atoms = true;
+  c->have_dtab = false;
   drop_graph(c);
   c->have_proj = total == 0;
   c->have_moments = false;
@@ -954,7 +961,62 @@ int sqb_moments_at(sqb_ctx *c, const double *chi, const double *zee, double *rho
   return SQB_OK;
 }
 
-int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff) {
+// Derivative tables dchi/dR_alpha of every replica's projectors: central
+// differences of the projector kernel at the replica positions +-eps along
+// each axis, the balls' grid centres held fixed (the nearest node does not
+// move for so small a step).  O(eps^2) = 1e-8 relative.
+static int ensure_dtab(sqb_ctx *c) {
+  if (c->have_dtab) return SQB_OK;
+  if (!c->have_tables) return SQB_ERR_STATE;
+  const long long T = c->tab_pad_total;
+  if (T == 0) {
+    c->have_dtab = true;
+    return SQB_OK;
+  }
+  if (c->d_dtab) cudaFree(c->d_dtab);
+  c->d_dtab = nullptr;
+  CK(dalloc(&c->d_dtab, (size_t)3 * T));
+  const size_t nr3 = (size_t)3 * c->n_rep;
+  int rc = ensure_tmp(c, (2 * (size_t)T + nr3) * sizeof(double));
+  if (rc) return rc;
+  double *plus = reinterpret_cast<double *>(c->d_tmp), *minus = plus + T, *xyz = minus + T;
+  const double eps = 1e-4;
+  std::vector<double> sh(nr3);
+  ProjArgs p{};
+  p.n_rep = c->n_rep;
+  p.delta = c->g.delta;
+  p.rep_nn = c->d_rep_nn;
+  p.rep_xyz = xyz;
+  p.rep_off = c->d_rep_off;
+  p.typ_nlocc = c->d_typ_nlocc;
+  p.typ_lmax = c->d_typ_lmax;
+  p.typ_lloc = c->d_typ_lloc;
+  p.typ_size = c->d_typ_size;
+  p.typ_tab = c->d_typ_tab;
+  p.tables = c->d_tables;
+  p.out32 = nullptr;
+  p.total = c->tab_total;
+  p.status = c->d_status;
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(plus, 0, 2 * (size_t)T * sizeof(double), c->stream));  // plane padding stays zero
+  for (int al = 0; al < 3; al++) {
+    for (int s = 0; s < 2; s++) {
+      sh = c->h_rep_xyz;
+      for (int r = 0; r < c->n_rep; r++) sh[3 * r + al] += s == 0 ? eps : -eps;
+      CK(cudaMemcpyAsync(xyz, sh.data(), nr3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      p.out64 = s == 0 ? plus : minus;
+      CK(launch_projectors(p, c->stream));
+      CK(cudaStreamSynchronize(c->stream));  // sh is reused
+    }
+    CK(launch_fd_combine(plus, minus, c->d_dtab + (size_t)al * T, T, 0.5 / eps, c->stream));
+  }
+  rc = read_status(c);
+  if (rc) return rc;
+  c->have_dtab = true;
+  return SQB_OK;
+}
+
+int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff, double *g_atoms) {
   if (!c || !g_mu || !g_veff) return SQB_ERR_ARG;
   if (!c->have_moments) return SQB_ERR_STATE;
   cudaSetDevice(c->device);
@@ -974,6 +1036,22 @@ int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff) {
     c->vjp_bytes = need;
   }
   double *d_scr = c->d_vjp, *d_g = d_scr + per * grid, *d_out = d_g + N * K;
+  const size_t per_at = (size_t)(4 * VJP_K + 12) * MAXP;  // doubles per CTA
+  double *d_gat = nullptr;
+  if (g_atoms) {
+    int rc0 = ensure_dtab(c);
+    if (rc0) return rc0;
+    const size_t need_at = (per_at * grid + (size_t)3 * std::max(c->n_atm, 1)) * sizeof(double);
+    if (c->vjp_at_bytes < need_at) {
+      if (c->d_vjp_at) cudaFree(c->d_vjp_at);
+      c->d_vjp_at = nullptr;
+      c->vjp_at_bytes = 0;
+      CK(cudaMalloc((void **)&c->d_vjp_at, need_at));
+      c->vjp_at_bytes = need_at;
+    }
+    d_gat = c->d_vjp_at + per_at * grid;
+    CK(cudaMemsetAsync(d_gat, 0, (size_t)3 * std::max(c->n_atm, 1) * sizeof(double), c->stream));
+  }
   CK(cudaMemcpyAsync(d_g, g_mu, N * K * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(d_out, 0, ext * sizeof(double), c->stream));
   NodeArgs a;
@@ -985,6 +1063,13 @@ int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff) {
   a.vjp = d_scr;
   a.vjp_stride = per;
   a.g_veff = d_out;
+  if (g_atoms) {
+    a.dtab = c->d_dtab;
+    a.dtab_stride = c->tab_pad_total;
+    a.g_atoms = d_gat;
+    a.vjp_at = c->d_vjp_at;
+    a.vjp_at_stride = per_at;
+  }
   CK(cudaEventRecord(c->ev0, c->stream));
   int rc = run_nodes(c, a, c->d_nodes, c->nnode);
   if (rc) return rc;
@@ -993,6 +1078,10 @@ int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff) {
   c->stats.ms_vjp = elapsed(c);
   if (rc) return rc;
   CK(cudaMemcpy(g_veff, d_out, ext * sizeof(double), cudaMemcpyDeviceToHost));
+  if (g_atoms && c->n_atm > 0) {
+    CK(cudaMemcpy(g_atoms, d_gat, (size_t)3 * c->n_atm * sizeof(double), cudaMemcpyDeviceToHost));
+    return reduce(c, g_atoms, 3 * c->n_atm, SQB_SUM);
+  }
   return SQB_OK;
 }
 

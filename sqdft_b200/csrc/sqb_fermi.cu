@@ -289,7 +289,7 @@ __global__ void proj_kernel(ProjArgs a) {
     const double u = UlJ * real_sh(xr, yr, zr, rad, l, m) * (VlJ - VlocJ);
     const long long o = a.rep_off[r] + ((long long)q * Sd + ctr / (Sd * Sd)) * plane_stride(Sd) + ctr % (Sd * Sd);
     a.out64[o] = u;
-    a.out32[o] = (float)u;
+    if (a.out32) a.out32[o] = (float)u;
   }
 }
 
@@ -334,6 +334,12 @@ __global__ void repack_kernel(const int *rep_nn, const int *typ_nlocc, const int
     if (to_pad) out[ip] = in[ir];
     else out[ir] = in[ip];
   }
+}
+
+// (plus - minus) * scale, element-wise (central differences of tables).
+__global__ void fd_combine_kernel(const double *plus, const double *minus, double *out, long long n, double scale) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (plus[i] - minus[i]) * scale;
 }
 
 __global__ void to_float_kernel(const double *in, float *out, long long n) {
@@ -399,6 +405,13 @@ cudaError_t launch_minmax(const double *lmin, const double *lmax, int n, double 
 cudaError_t launch_to_float(const double *in, float *out, long long n, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   to_float_kernel<<<296, 256, 0, s>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fd_combine(const double *plus, const double *minus, double *out, long long n, double scale,
+                              cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  fd_combine_kernel<<<296, 256, 0, s>>>(plus, minus, out, n, scale);
   return cudaGetLastError();
 }
 

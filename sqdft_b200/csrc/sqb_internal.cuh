@@ -86,6 +86,14 @@ struct NodeArgs {
   double *vjp;
   size_t vjp_stride;  // doubles per CTA
   double *g_veff;
+  // MODE_VJP with atom gradients: derivative tables dchi/dR_alpha (3 x the
+  // padded tables, stride dtab_stride values), dL/dR per atom [n_atm][3]
+  // (type-major, the layout of the forces), per-CTA scratch vjp_at
+  const double *dtab;
+  long long dtab_stride;
+  double *g_atoms;
+  double *vjp_at;
+  size_t vjp_at_stride;  // doubles per CTA
   int *status;
   unsigned long long *proj_points; // algorithmic projector-ball points touched
 };
@@ -134,12 +142,15 @@ struct ProjArgs {
   const long long *typ_tab; // offset of each type's 19 x size tables
   const double *tables;
   double *out64;
-  float *out32;
+  float *out32;  // may be NULL (no FP32 copy)
   long long total;
   int *status;
 };
 cudaError_t launch_projectors(const ProjArgs &a, cudaStream_t s);
 cudaError_t launch_to_float(const double *in, float *out, long long n, cudaStream_t s);
+// out = (plus - minus) * scale, element-wise.
+cudaError_t launch_fd_combine(const double *plus, const double *minus, double *out, long long n, double scale,
+                              cudaStream_t s);
 // Copy tables between the reference's UdVtm layout and the padded device layout.
 cudaError_t launch_repack(int n_rep, const int *rep_nn, const int *typ_nlocc, const int *typ_nproj,
                           const long long *off_ref, const long long *off_pad, const double *in, double *out,

@@ -115,6 +115,9 @@ struct PassIO {
   int dbl = 0;                  // accumulate the doubling dot products
   T *wout = nullptr;            // PK_LZF: where the formed input is stored
   int konst = 0;                // PK_LZF: the input is the constant sin
+  double *pg = nullptr;         // adjoint with atom gradients: dots with dchi/dR_alpha, [3][MAXP]
+  const double *dtab = nullptr; // dchi/dR tables (3 x stride values)
+  long long dstride = 0;
 };
 
 template <typename T>
@@ -360,8 +363,23 @@ __device__ __forceinline__ double box_dot(const T *pl, int pitch, const T *U, in
 }
 
 template <typename T>
+__device__ __forceinline__ double box_dot_d(const T *pl, int pitch, const double *U, int Sd, int bx, int by, int lane) {
+  double acc = 0.0;
+  const RowLanes L(bx, lane);
+  if (L.lr < L.R) {
+    for (int y = L.lr; y < by; y += L.R)
+      for (int x = L.lx; x < bx; x += L.W) acc += (double)pl[y * pitch + x] * U[y * Sd + x];
+  }
+  return acc;
+}
+
+// pg != nullptr (adjoint with atom gradients): also the dot products with the
+// derivative tables dchi/dR_alpha of every crossing box, added to pg[alpha][p]
+// (read from global memory: this runs only in the adjoint kernel group).
+template <typename T>
 __device__ void dot_phase(NodeShared &S, const T *plane, int zz, int pitch, const T *tab, const short *offz,
-                          const unsigned char *crossz, const T *stage) {
+                          const unsigned char *crossz, const T *stage, double *pg = nullptr,
+                          const double *dtab = nullptr, long long dstride = 0) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int k = warp; k < S.ncross[zz]; k += nw) {
     const int e = crossz[k];
@@ -384,6 +402,15 @@ __device__ void dot_phase(NodeShared &S, const T *plane, int zz, int pitch, cons
       }
       acc = warp_sum(acc);
       if (lane == 0) S.p_nxt[pb + q] += acc;
+      if (pg) {
+        const double *Ud = dtab + S.e_tab[e] + (long long)(q * Sd + S.e_tz0[e] + zz) * S.e_sp2[e] + r0;
+#pragma unroll
+        for (int al = 0; al < 3; al++) {
+          double ad = box_dot_d<T>(pl, pitch, Ud + al * dstride, Sd, bx, by, lane);
+          ad = warp_sum(ad);
+          if (lane == 0) pg[al * MAXP + pb + q] += ad;
+        }
+      }
     }
   }
 }
@@ -545,7 +572,7 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
     __syncthreads();
     if (DOTS && z >= 1 && S.n_ent > 0)
       dot_phase<T>(S, sm_out + ((z - 1) & 1) * n2, z - 1, n, tab, off_tab + (z - 1) * MAXE,
-                   cross_list(a, dyn) + (z - 1) * MAXE, stage_ptr<T>(a, dyn, st_prev));
+                   cross_list(a, dyn) + (z - 1) * MAXE, stage_ptr<T>(a, dyn, st_prev), io.pg, io.dtab, io.dstride);
     if (staged && z + 1 < n) issue_plane<T>(a, S, dyn, z + 1, st_next);
     if (z == n) break;
     // Nonlocal gather: the boxes covering this warp's rows and crossing plane
@@ -809,7 +836,7 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
     __syncthreads();
     if (DOTS && z >= 1 && S.n_ent > 0)
       dot_phase<T>(S, sm_out + ((z - 1) & 1) * OPLANE, z - 1, 32, tab, off_tab + (z - 1) * MAXE,
-                   cross_list(a, dyn) + (z - 1) * MAXE, stage_ptr<T>(a, dyn, st_prev));
+                   cross_list(a, dyn) + (z - 1) * MAXE, stage_ptr<T>(a, dyn, st_prev), io.pg, io.dtab, io.dstride);
     if (staged && z + 1 < n) issue_plane<T>(a, S, dyn, z + 1, st_next);
     if (z == n) break;
 
@@ -1548,25 +1575,53 @@ __device__ void node_forces(const NodeArgs &a, NodeShared &S, unsigned char *dyn
 
 // Gradient of L = sum_j g_j mu_j (mu_j = e_c^T T_j(Ht) e_c / h^3, the node's
 // Chebyshev moments, Ht = (H - chi)/zee with chi, zee held fixed) with respect
-// to Veff on the node's window, added into a.g_veff.  Forward recursion
-// t_0 = e_c, t_1 = Ht t_0, t_k+1 = 2 Ht t_k - t_k-1 (sq.cpp:579-616) with the
-// pair (t_sK, t_sK+1) and the projections of t_sK+1 checkpointed every K
-// steps; reverse Clenshaw recursion a_k = (g_k/h^3) e_c + 2 Ht a_k+1 - a_k+2
-// from k = npl down to 1, segment by segment, recomputing each segment's
-// vectors from its checkpoint; dL/dHt_xx = a_1 t_0 + 2 sum_k a_k+1 t_k, and
-// dL/dVeff(x) = dL/dHt_xx / zee.
+// to Veff on the node's window, added into a.g_veff, and (a.g_atoms set) with
+// respect to the replica positions through the projectors, added into the
+// gradient of each replica's atom.  Forward recursion t_0 = e_c, t_1 = Ht t_0,
+// t_k+1 = 2 Ht t_k - t_k-1 (sq.cpp:579-616) with the pair (t_sK, t_sK+1) and
+// the projections of t_sK+1 checkpointed every K steps; reverse Clenshaw
+// recursion a_k = (g_k/h^3) e_c + 2 Ht a_k+1 - a_k+2 from k = npl down to 1,
+// segment by segment, recomputing each segment's vectors from its checkpoint;
+// dL/dHt = a_1 t_0^T + 2 sum_k a_k+1 t_k^T, so
+//   dL/dVeff(x) = (a_1 t_0 + 2 sum_k a_k+1 t_k)(x) / zee and, with
+//   dVnl/dR = sum_q (dchi_q chi_q^T + chi_q dchi_q^T) / Denom_q,
+//   dL/dR = sum_k c_k sum_q [(a_k+1.dchi_q)(chi_q.t_k) + (a_k+1.chi_q)(dchi_q.t_k)]
+//           / (Denom_q zee),  c_k = 2 (k >= 1), 1 (k = 0).
 template <int C>
 __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const uint32_t (&mask)[4],
                          double chi, double zee, const double *g) {
   const int n = a.n, npl = a.npl, K = VJP_K, nseg = (npl + K - 1) / K;
   const size_t nw = (size_t)n * n * n;
+  const bool at = a.g_atoms != nullptr;
   double *ck = a.vjp + (size_t)blockIdx.x * a.vjp_stride;  // [nseg][2][nw]
   double *seg = ck + (size_t)nseg * 2 * nw;                  // [K][nw]
   double *A = seg + (size_t)K * nw;                          // [3][nw]
   double *G = A + 3 * nw;                                    // [nw]
   double *ckp = G + nw;                                      // [nseg][MAXP]
+  // atom gradients: chi / dchi dots of the segment's t ([K][MAXP], [K][3][MAXP]),
+  // dchi dots of a_k+1 (pgA), of the output being formed (pgN), saved (pgS),
+  // and the per-projector sums (dRp)
+  double *Tt = at ? a.vjp_at + (size_t)blockIdx.x * a.vjp_at_stride : nullptr;
+  double *Tg = at ? Tt + (size_t)K * MAXP : nullptr;
+  double *pgA = at ? Tg + (size_t)3 * K * MAXP : nullptr;
+  double *pgN = at ? pgA + 3 * MAXP : nullptr, *pgS = at ? pgN + 3 * MAXP : nullptr;
+  double *dRp = at ? pgS + 3 * MAXP : nullptr;
+  const int npi = S.n_pi;
   double d0 = 0.0, d1 = 0.0;
   for (size_t i = threadIdx.x; i < nw; i += blockDim.x) G[i] = 0.0;
+  if (at)
+    for (int i = threadIdx.x; i < 3 * MAXP; i += blockDim.x) {
+      dRp[i] = 0.0;
+      pgN[i] = 0.0;
+    }
+  __syncthreads();
+  auto gradio = [&](PassIO<double> &io) {
+    if (at) {
+      io.pg = pgN;
+      io.dtab = a.dtab;
+      io.dstride = a.dtab_stride;
+    }
+  };
   // forward: checkpoints only
   {
     PassIO<double> io;
@@ -1582,7 +1637,7 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
     io.cb = zee;
     run_pass<double, C, PK_CH1>(a, S, dyn, io, mask, d0, d1);
     rotate_proj(S, 1.0);
-    for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) ckp[p] = S.p_cur[p];
+    for (int p = threadIdx.x; p < npi; p += blockDim.x) ckp[p] = S.p_cur[p];
   }
   const double *tm1 = ck, *tk = ck + nw;
   for (int k = 1; k + 1 <= npl - 1; k++) {
@@ -1597,10 +1652,17 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
     run_pass<double, C, PK_CH>(a, S, dyn, io, mask, d0, d1);
     rotate_proj(S, 1.0);
     if (r == 1)
-      for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) ckp[(size_t)sg * MAXP + p] = S.p_cur[p];
+      for (int p = threadIdx.x; p < npi; p += blockDim.x) ckp[(size_t)sg * MAXP + p] = S.p_cur[p];
     tm1 = tk;
     tk = out;
   }
+  // dchi dots of the output just formed -> dst (scaled), pgN cleared
+  auto take_pg = [&](double *dst, double scale) {
+    for (int i = threadIdx.x; i < 3 * MAXP; i += blockDim.x) {
+      dst[i] = scale * pgN[i];
+      pgN[i] = 0.0;
+    }
+  };
   // backward: a_npl = (g_npl / h^3) e_c (stored as e_c with a lazy scale), a_npl+1 = 0
   const double h3 = a.h3;
   double *an1 = A, *an2 = A, *afree = A + nw, *aspare = A + 2 * nw;
@@ -1608,8 +1670,11 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
   {
     PassIO<double> io;
     io.out = A;
+    gradio(io);
     run_pass<double, C, PK_DELTA>(a, S, dyn, io, mask, d0, d1);
     rotate_proj(S, sc1);
+    if (at) take_pg(pgA, sc1);
+    __syncthreads();
   }
   for (int sg = nseg - 1; sg >= 0; sg--) {
     const int lo = sg * K, hi = min(lo + K - 1, npl - 1);
@@ -1618,10 +1683,31 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
     tv[0] = ck + (size_t)(2 * sg) * nw;
     if (hi >= lo + 1) tv[1] = ck + (size_t)(2 * sg + 1) * nw;
     for (int j = 2; j < K; j++) tv[j] = seg + j * nw;
-    if (hi >= lo + 2) {
-      // recompute t_lo+2 .. t_hi, keeping the adjoint's projections aside
-      for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) {
-        S.pw_prev[p] = S.p_cur[p];
+    const bool recompute = hi >= lo + 2;
+    if (recompute || at) {
+      // keep the adjoint's projections aside
+      for (int p = threadIdx.x; p < npi; p += blockDim.x) S.pw_prev[p] = S.p_cur[p];
+      if (at)
+        for (int i = threadIdx.x; i < 3 * MAXP; i += blockDim.x) pgS[i] = pgA[i];
+      __syncthreads();
+    }
+    if (at) {
+      // chi and dchi dots of the checkpointed t_lo, t_lo+1
+      for (int j = 0; j < 2 && lo + j <= hi; j++) {
+        for (int p = threadIdx.x; p < npi; p += blockDim.x) S.p_nxt[p] = 0.0;
+        __syncthreads();
+        PassIO<double> io;
+        io.din = tv[j];
+        gradio(io);
+        run_pass<double, C, PK_DOTS>(a, S, dyn, io, mask, d0, d1);
+        for (int p = threadIdx.x; p < npi; p += blockDim.x) Tt[(size_t)j * MAXP + p] = S.p_nxt[p];
+        take_pg(Tg + (size_t)j * 3 * MAXP, 1.0);
+        __syncthreads();
+      }
+    }
+    if (recompute) {
+      // recompute t_lo+2 .. t_hi from the checkpoint
+      for (int p = threadIdx.x; p < npi; p += blockDim.x) {
         S.p_cur[p] = ckp[(size_t)sg * MAXP + p];
         S.p_nxt[p] = 0.0;
       }
@@ -1633,13 +1719,22 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
         io.out = seg + (size_t)(k + 1 - lo) * nw;
         io.ca = chi;
         io.cb = zee;
+        gradio(io);
         run_pass<double, C, PK_CH>(a, S, dyn, io, mask, d0, d1);
+        if (at) {
+          for (int p = threadIdx.x; p < npi; p += blockDim.x) Tt[(size_t)(k + 1 - lo) * MAXP + p] = S.p_nxt[p];
+          take_pg(Tg + (size_t)(k + 1 - lo) * 3 * MAXP, 1.0);
+        }
         rotate_proj(S, 1.0);
       }
-      for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) {
+    }
+    if (recompute || at) {
+      for (int p = threadIdx.x; p < npi; p += blockDim.x) {
         S.p_cur[p] = S.pw_prev[p];
         S.p_nxt[p] = 0.0;
       }
+      if (at)
+        for (int i = threadIdx.x; i < 3 * MAXP; i += blockDim.x) pgA[i] = pgS[i];
       __syncthreads();
     }
     for (int k = hi; k >= lo && k >= 1; k--) {
@@ -1658,7 +1753,20 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
       io.cd = g[k] / h3;
       io.ce = 2.0;
       io.dacc = G;
+      gradio(io);
       run_pass<double, C, PK_ADJ>(a, S, dyn, io, mask, d0, d1);
+      if (at) {
+        // step k's term: a_k+1 (projections in p_cur, dchi dots in pgA) with t_k
+        for (int p = threadIdx.x; p < npi; p += blockDim.x) {
+          const double D = S.p_den[p], Ak = S.p_cur[p] * D, Tk = Tt[(size_t)(k - lo) * MAXP + p];
+#pragma unroll
+          for (int al = 0; al < 3; al++)
+            dRp[al * MAXP + p] +=
+                2.0 * (pgA[al * MAXP + p] * Tk + Ak * Tg[((size_t)(k - lo) * 3 + al) * MAXP + p]) / D;
+        }
+        __syncthreads();
+        take_pg(pgA, 1.0);
+      }
       rotate_proj(S, 1.0);
       if (out == afree) {
         afree = aspare;
@@ -1671,8 +1779,15 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
     }
   }
   __syncthreads();
-  // a_1 t_0 (t_0 = e_c): the last step's centre value
+  // a_1 t_0 (t_0 = e_c): the last step's centre value; for the atoms, a_1
+  // with t_0's dots (segment 0, kept in Tt[0], Tg[0])
   if (threadIdx.x == 0) G[(size_t)(a.nloc * n + a.nloc) * n + a.nloc] += S.center_val;
+  if (at)
+    for (int p = threadIdx.x; p < npi; p += blockDim.x) {
+      const double D = S.p_den[p], A1 = S.p_cur[p] * D, T0 = Tt[p];
+#pragma unroll
+      for (int al = 0; al < 3; al++) dRp[al * MAXP + p] += (pgA[al * MAXP + p] * T0 + A1 * Tg[al * MAXP + p]) / D;
+    }
   __syncthreads();
   // dL/dVeff on the block with halo: the window of node (gi, gj, gk) starts at
   // (gi, gj, gk) in the halo'd block
@@ -1682,6 +1797,14 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
     const size_t ve = ((size_t)(S.gk + z) * a.ey + (S.gj + y)) * a.ex + (S.gi + x);
     atomicAdd(&a.g_veff[ve], G[i] * iz);
   }
+  // dL/dR: each box's projectors summed into its replica's atom
+  if (at)
+    for (int i = threadIdx.x; i < S.n_ent * 3; i += blockDim.x) {
+      const int e = i / 3, al = i % 3;
+      double sum = 0.0;
+      for (int q = 0; q < S.e_np[e]; q++) sum += dRp[al * MAXP + S.e_pb[e] + q];
+      atomicAdd(&a.g_atoms[(size_t)S.e_atom[e] * 3 + al], sum * iz);
+    }
   count_proj_points(a, S, 2 * npl, 1);
 }
 

@@ -102,7 +102,7 @@ def library() -> C.CDLL:
         lib.sqb_moments_at.argtypes = [P, _dp, _dp, _dp]
         lib.sqb_autotune.argtypes = [P, C.c_int, _ip, _dp]
         lib.sqb_set_graph.argtypes = [P, C.c_int]
-        lib.sqb_moments_vjp.argtypes = [P, _dp, _dp]
+        lib.sqb_moments_vjp.argtypes = [P, _dp, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
         lib.sqb_version.restype = C.c_char_p
@@ -271,14 +271,15 @@ class Context:
         _check(self.lib.sqb_moments_at(self.ptr, _d(chi), _d(zee), _d(rho_pj)), "sqb_moments_at")
         return rho_pj
 
-    def moments_vjp(self, g_mu: np.ndarray) -> np.ndarray:
+    def moments_vjp(self, g_mu: np.ndarray, atoms: bool = False):
         """dL/dVeff on the Veff block with halo for dL/drho_pj = g_mu (bounds of the
-        last moments held fixed)."""
+        last moments held fixed); with atoms=True also dL/dR [n_atm][3]."""
         c = self.case
         g = np.ascontiguousarray(g_mu, np.float64).reshape(c.n_nodes, c.npl + 1)
         out = np.zeros(self._veff_ext_shape())
-        _check(self.lib.sqb_moments_vjp(self.ptr, _d(g), _d(out)), "sqb_moments_vjp")
-        return out
+        gat = np.zeros((c.n_atm, 3)) if atoms else None
+        _check(self.lib.sqb_moments_vjp(self.ptr, _d(g), _d(out), _d(gat)), "sqb_moments_vjp")
+        return (out, gat) if atoms else out
 
     def ne_constraint(self, lam: float) -> float:
         v = C.c_double()
