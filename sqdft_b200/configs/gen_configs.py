@@ -79,6 +79,14 @@ SYSTEMS = {
     "al_ref": System("al_ref", 7.78, 1, 10, 46418.02 * KB_EV, 28, 6.0, 0.0, 0, _al_basis(),
                      note="reference regression Al, 4 atoms, 17^3 window",
                      xyz=((0.0, 0.0, 0.0), (0.0, 3.89, 3.89), (3.89, 0.0, 3.89), (3.74, 3.49, 0.37))),
+    # The same geometry on finer grids at npl 64: the adjoint's atom gradient
+    # against the reference's nonlocal forces as the grid is refined.
+    "al_ref14": System("al_ref14", 7.78, 1, 14, 46418.02 * KB_EV, 64, 6.0, 0.0, 0, _al_basis(),
+                       note="reference regression Al geometry, 14^3 grid, 23^3 window",
+                       xyz=((0.0, 0.0, 0.0), (0.0, 3.89, 3.89), (3.89, 0.0, 3.89), (3.74, 3.49, 0.37))),
+    "al_ref20": System("al_ref20", 7.78, 1, 20, 46418.02 * KB_EV, 64, 6.0, 0.0, 0, _al_basis(),
+                       note="reference regression Al geometry, 20^3 grid, 33^3 window",
+                       xyz=((0.0, 0.0, 0.0), (0.0, 3.89, 3.89), (3.89, 0.0, 3.89), (3.74, 3.49, 0.37))),
 }
 
 

@@ -273,3 +273,40 @@ def test_atom_gradient_matches_central_differences(name):
                 vals.append(float(np.sum(g * ctx.moments_at(chi, zee))))
             fd = (vals[0] - vals[1]) / (2 * eps)
             assert abs(fd - gat[atom, al]) <= 1e-5 * scale, (atom, al, fd, gat[atom, al], scale)
+
+
+def _nonlocal_force_gap(name):
+    """max|(-dOmega_band/dR) - F_nonlocal| and max|F_nonlocal| on one system:
+    the adjoint's atom gradient of the band grand potential (Veff, bounds and
+    Fermi level fixed) against the force of ForcesNonLocal (forces.cpp:318)."""
+    from sqdft_b200 import sq
+    from sqdft_b200.cases import load
+
+    case = load(name)
+    h3 = case.delta ** 3
+    with sq.Context(case, device=0) as ctx:
+        ctx.nonlocal_projectors()
+        out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+        f = ctx.forces_nonlocal()
+        m = ctx.lanczos_moments()
+        d = _grand_potential_coeffs(m["chi"], m["zee"], out["lambda_f"], case.bet, case.npl)
+        ctx.moments_at(m["chi"], m["zee"])
+        _, gat = ctx.moments_vjp(2.0 * h3 * d, atoms=True)
+    return float(np.abs(gat + f).max()), float(np.abs(f).max())
+
+
+def test_atom_gradient_converges_to_reference_nonlocal_forces():
+    """-dOmega_band/dR is the nonlocal Hellmann-Feynman force.  ForcesNonLocal
+    moves the position derivative onto the density-matrix column as its
+    12th-order grid gradient (summation by parts), the adjoint differentiates
+    the grid-sampled projector itself; the two differ by the grid's
+    translation error, which vanishes with the spacing.  On the regression Al
+    geometry (npl 64, Rcut 6; measured on B200) the gap is 0.164 of max|F| at
+    h = 0.556 and 0.052 at h = 0.389, while a 4 -> 8 bohr window or npl
+    32 -> 128 moves it by under 0.07."""
+    gap14, f14 = _nonlocal_force_gap("al_ref14")
+    gap20, f20 = _nonlocal_force_gap("al_ref20")
+    print(f"nonlocal force gap: h=0.556 {gap14 / f14:.3e}, h=0.389 {gap20 / f20:.3e}")
+    assert abs(f20 - f14) <= 0.05 * f20  # the same physical force on both grids
+    assert gap20 <= 0.08 * f20
+    assert gap20 <= 0.45 * gap14
