@@ -7,13 +7,17 @@ Fermi-level solve, density and energies.  The default workload is the
 Chebyshev order 96) with the reference's own first-SCF-iteration Veff.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2]
-                    [--precision fp64|mixed] [--impl ours|reference]
+                    [--precision fp64|mixed] [--mixed-lanczos-tol T]
+                    [--impl ours|reference]
 
 value  nodes / (device time of the step), inputs resident in HBM
 e2e    nodes / (wall time of the C-ABI call with host buffers: Veff copied
        in from pinned memory, rho, rho_pj, Ci, chi, zee copied out)
 With N > 1 (torchrun, NCCL), rank r owns a z-slab of the grid; the
 Fermi-level sums and energies are all-reduced through the library's hook.
+--precision mixed runs the FP32-mixed path (FP32 Lanczos vectors with the
+Lanczos stop at T Ha, FP64 moments) and, outside the timed region, one FP64
+step of the same input to state the density error against it.
 --impl reference times the reference SQDFT compiled from its sources
 (oracle/_ref/sqref_driver: its LanczosAlgorithm and HsubTimesVec per node)
 on a node sample across all host threads.
@@ -100,14 +104,16 @@ def dist_env():
 def algorithmic_bytes(stats, case, precision):
     """Bytes per node-kernel launch by the roofline's accounting: per matvec
     step n_w (3 s_v + s_V) plus the projector tables of every atom whose ball
-    meets the window, steps = Lanczos iterations + 1 + npl/2 per node."""
+    meets the window, steps = Lanczos iterations + 1 + npl/2 per node.  Veff
+    and the tables are FP64 in both paths; the Lanczos vectors (s_v) are FP32
+    in the mixed path, the Chebyshev vectors FP64 in both."""
     nw = stats["window_points"]
     n = case.n_nodes
     lz_steps = stats["lanczos_iters"] + n
     ch_steps = n * (case.npl // 2)
-    sv = 8 if precision == 0 else 4
+    sv_lz = 8 if precision == 0 else 4
     proj_lz = stats["proj_points"] - stats["proj_points_cheb"]
-    return (lz_steps * nw * 32 + proj_lz * 8) + (ch_steps * nw * 4 * sv + stats["proj_points_cheb"] * sv)
+    return (lz_steps * nw * (3 * sv_lz + 8) + proj_lz * 8) + (ch_steps * nw * 32 + stats["proj_points_cheb"] * 8)
 
 
 def run_ours(args):
@@ -127,6 +133,8 @@ def run_ours(args):
     prec = sq.SQB_FP64 if args.precision == "fp64" else sq.SQB_FP32_MIXED
 
     ctx = sq.Context(my, device=local, precision=prec, allreduce=allreduce_fn(dist, "cuda") if ws > 1 else None)
+    if prec == sq.SQB_FP32_MIXED:
+        ctx.set_mixed_lanczos_tol(args.mixed_lanczos_tol)
     ctx.nonlocal_projectors()
     n = my.n_nodes
     K1 = my.npl + 1
@@ -139,6 +147,8 @@ def run_ours(args):
     import ctypes as C
 
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+
+    st_ebs = [0.0]
 
     def step():
         flush.fill_(1)  # evict L2 (126 MB) between steps
@@ -156,6 +166,7 @@ def run_ours(args):
             raise sq.SQBError(rc, "sqb_spectral_quadrature")
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+        st_ebs[0] = ebs.value
         st = ctx.stats()
         dev_ms = st["ms_lanczos_moments"] + st["ms_fermi"] + st["ms_density"]
         return wall, dev_ms, st, lamv.value
@@ -177,6 +188,19 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         wall, dev, kern = t.tolist()
     st = ctx.stats()
+    accuracy = None
+    if prec == sq.SQB_FP32_MIXED:  # untimed: the FP64 step on the same input
+        rho_mixed, lam_mixed, ebs_mixed = outs["rho"].copy(), lam, st_ebs[0]
+        ctx.set_precision(sq.SQB_FP64)
+        ref = ctx.spectral_quadrature(1, case.lambda_f)
+        ctx.set_precision(prec)
+        t = torch.tensor([np.abs(rho_mixed - ref["rho"].reshape(-1)).max(), np.abs(ref["rho"]).max()],
+                         dtype=torch.float64, device="cuda")
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        accuracy = {"rho_rel_err_vs_fp64": float(t[0] / t[1]), "lambda_f_diff": abs(lam_mixed - ref["lambda_f"]),
+                    "ebs_diff_per_atom": abs(ebs_mixed - ref["Ebs"]) / case.n_atm,
+                    "mixed_lanczos_tol": args.mixed_lanczos_tol}
     traffic_per_node_step = None
     tr = ROOT / "profiles" / "node_kernel_traffic.json"
     if tr.exists():
@@ -193,7 +217,8 @@ def run_ours(args):
         cpu = cpu_baseline(args) if (ws == 1 and not args.no_cpu) else None
         res = {
             "metric": "SQ grid nodes/s (FP64 SQ step: Lanczos + Chebyshev moments + Fermi level + density)"
-            if prec == 0 else "SQ grid nodes/s (FP32-mixed SQ step)",
+            if prec == 0 else "SQ grid nodes/s (FP32-mixed SQ step: FP32 Lanczos vectors and a looser Lanczos "
+            "stop, FP64 moments + Fermi level + density)",
             "value": nodes / dev, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dev * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64" if prec == 0 else "f32-mixed", "data": "synthetic (seeded-Gaussian-displaced FCC Al; "
@@ -213,6 +238,8 @@ def run_ours(args):
             "lanczos_iters_per_node": st["lanczos_iters"] / n, "fermi_iters": st["fermi_iters"],
             "lambda_f": lam,
         }
+        if accuracy:
+            res["accuracy"] = accuracy
         if cpu:
             res["cpu_baseline"] = cpu
     ctx.close()
@@ -289,6 +316,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c2")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--mixed-lanczos-tol", type=float, default=1e-3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")

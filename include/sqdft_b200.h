@@ -40,10 +40,14 @@ extern "C" {
 #define SQB_ERR_NONFINITE 11       /* NaN or Inf met in inputs or in a result */
 #define SQB_ERR_STATE 12           /* entry point called before its inputs were set */
 
-/* Arithmetic of the recursion vectors (Chebyshev and Lanczos). */
+/* Precision of the recursion vectors (Chebyshev and Lanczos). */
 #define SQB_FP64 0        /* everything in FP64: parity path */
-#define SQB_FP32_MIXED 1  /* FP32 Chebyshev vectors and stencil, FP64 moments,
-                             Lanczos bounds, coefficients, Fermi solve, assembly */
+#define SQB_FP32_MIXED 1  /* Lanczos vectors (and the nonlocal-force recursion
+                             vectors) stored in FP32, stencil arms summed in FP32;
+                             Veff, projector tables, the rest of the arithmetic,
+                             the Chebyshev moments, coefficients, Fermi solve and
+                             assembly in FP64.  Lanczos stops at
+                             max(lanczos_tol, sqb_set_mixed_lanczos_tol). */
 
 typedef struct sqb_ctx sqb_ctx;
 
@@ -110,6 +114,12 @@ typedef struct sqb_stats {
 int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out);
 int sqb_destroy(sqb_ctx *ctx);
 int sqb_set_precision(sqb_ctx *ctx, int precision);
+/* Lanczos stopping tolerance (Ha) of the FP32-mixed path, also the margin
+ * put around its Ritz values (sq.cpp:1050-1092 with this tolerance); default
+ * 0, i.e. sqb_grid.lanczos_tol.  The density's sensitivity to the bounds
+ * falls with npl: a looser stop suits high-order expansions only.  The FP64
+ * path always uses sqb_grid.lanczos_tol.  No counterpart in the reference. */
+int sqb_set_mixed_lanczos_tol(sqb_ctx *ctx, double tol);
 int sqb_set_allreduce(sqb_ctx *ctx, sqb_allreduce_fn fn, void *user);
 /* Launch shape of the node kernel: persistent CTAs per SM, and the layout of
  * its plane loop: window columns per thread (1 or 2; 0 = automatic, one

@@ -25,6 +25,7 @@ struct sqb_ctx {
   int device = 0, sms = 148;
   cudaStream_t stream = nullptr;
   int precision = SQB_FP64;
+  double mixed_lanczos_tol = 0.0;  // Ha: the mixed path's Lanczos stop and margin (0: the grid's)
   int cols = 0, ctas_per_sm = 1;
   int use_graph = 0;                       // replay the node-kernel sequence from a CUDA graph
   cudaGraphExec_t sq_graph = nullptr;      // captured Lanczos+moments sequence (node kernel, min/max)
@@ -35,7 +36,6 @@ struct sqb_ctx {
   void *allreduce_user = nullptr;
 
   double *d_veff64 = nullptr;
-  float *d_veff32 = nullptr;
   bool have_veff = false;
 
   int n_typ = 0, n_rep = 0, n_atm = 0;
@@ -47,7 +47,6 @@ struct sqb_ctx {
   double *d_proj_denom = nullptr, *d_tables = nullptr, *d_rep_xyz = nullptr;
   bool have_tables = false;
   double *d_tab64 = nullptr;
-  float *d_tab32 = nullptr;
   long long tab_total = 0;      // values of the reference's UdVtm
   long long tab_pad_total = 0;  // values of the padded device tables
   long long *d_rep_off_ref = nullptr;
@@ -158,13 +157,13 @@ void fill_node_args(sqb_ctx *c, NodeArgs &a) {
   a.ey = c->ey;
   a.npl = c->g.npl;
   a.h3 = c->h3;
-  a.lanczos_tol = c->g.lanczos_tol;
+  a.mixed = c->precision == SQB_FP32_MIXED;
+  a.lanczos_tol = a.mixed ? std::max(c->g.lanczos_tol, c->mixed_lanczos_tol) : c->g.lanczos_tol;
   for (int k = 0; k <= FDN; k++) {
     a.coeff_lap[k] = c->g.coeff_lap[k];
     a.coeff_grad[k] = c->g.coeff_grad[k];
   }
   a.veff64 = c->d_veff64;
-  a.veff32 = c->d_veff32;
   a.at.n_rep = c->n_rep;
   a.at.rep_nn = c->d_rep_nn;
   a.at.rep_atom = c->d_rep_atom;
@@ -173,10 +172,8 @@ void fill_node_args(sqb_ctx *c, NodeArgs &a) {
   a.at.typ_nproj = c->d_typ_nproj;
   a.at.proj_denom = c->d_proj_denom;
   a.at.tab64 = c->d_tab64;
-  a.at.tab32 = c->d_tab32;
   a.counter = c->d_counter;
   a.status = c->d_status;
-  a.mixed = c->precision == SQB_FP32_MIXED;
   a.proj_points = c->d_proj_points;
   a.stage_bytes = node_kernel_stage_bytes(c->n, c->stage_elems);
 }
@@ -461,9 +458,9 @@ int sqb_destroy(sqb_ctx *c) {
   if (!c) return SQB_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void *ptrs[] = {c->d_veff64, c->d_veff32, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
+  void *ptrs[] = {c->d_veff64, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
                   c->d_typ_nlocc, c->d_typ_nproj, c->d_typ_lmax, c->d_typ_lloc, c->d_typ_size, c->d_proj_denom,
-                  c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_tab32, c->d_scratch, c->d_counter, c->d_nodes,
+                  c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
                   c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
                   c->d_f, c->d_tmp};
@@ -480,6 +477,13 @@ int sqb_destroy(sqb_ctx *c) {
 int sqb_set_precision(sqb_ctx *c, int precision) {
   if (!c || (precision != SQB_FP64 && precision != SQB_FP32_MIXED)) return SQB_ERR_ARG;
   c->precision = precision;
+  drop_graph(c);
+  return SQB_OK;
+}
+
+int sqb_set_mixed_lanczos_tol(sqb_ctx *c, double tol) {
+  if (!c || !(tol >= 0.0) || !std::isfinite(tol)) return SQB_ERR_ARG;
+  c->mixed_lanczos_tol = tol;
   drop_graph(c);
   return SQB_OK;
 }
@@ -509,12 +513,8 @@ int sqb_set_veff(sqb_ctx *c, const double *veff_ext) {
   const size_t n = (size_t)c->ex * c->ey * c->ez;
   for (size_t i = 0; i < n; i++)
     if (!std::isfinite(veff_ext[i])) return SQB_ERR_NONFINITE;
-  if (!c->d_veff64) {
-    CK(dalloc(&c->d_veff64, n));
-    CK(dalloc(&c->d_veff32, n));
-  }
+  if (!c->d_veff64) CK(dalloc(&c->d_veff64, n));
   CK(cudaMemcpyAsync(c->d_veff64, veff_ext, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(launch_to_float(c->d_veff64, c->d_veff32, (long long)n, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_veff = true;
   c->have_moments = false;
@@ -585,9 +585,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
   CK(dalloc(&c->d_typ_tab, std::max(n_typ, 1)));
   CK(dalloc(&c->d_proj_denom, denom.size()));
   CK(dalloc(&c->d_tab64, (size_t)std::max(total_pad, 1LL)));
-  CK(dalloc(&c->d_tab32, (size_t)std::max(total_pad, 1LL)));
   CK(cudaMemset(c->d_tab64, 0, (size_t)std::max(total_pad, 1LL) * sizeof(double)));
-  CK(cudaMemset(c->d_tab32, 0, (size_t)std::max(total_pad, 1LL) * sizeof(float)));
   CK(dalloc(&c->d_fslots, (size_t)c->nnode * FSLOTS * 4));
   CK(dalloc(&c->d_f, (size_t)3 * std::max(n_atm, 1)));
   CK(cudaMemcpy(c->d_rep_nn, nn.data(), nn.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -650,7 +648,6 @@ int sqb_nonlocal_projectors(sqb_ctx *c, double *udvtm_out) {
   p.typ_tab = c->d_typ_tab;
   p.tables = c->d_tables;
   p.out64 = c->d_tab64;
-  p.out32 = c->d_tab32;
   p.total = c->tab_total;
   p.status = c->d_status;
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
@@ -685,7 +682,6 @@ int sqb_set_projectors(sqb_ctx *c, const double *udvtm) {
     CK(cudaMemcpyAsync(d_ref, udvtm, (size_t)c->tab_total * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(launch_repack(c->n_rep, c->d_rep_nn, c->d_typ_nlocc, c->d_typ_nproj, c->d_rep_off_ref, c->d_rep_off, d_ref,
                      c->d_tab64, 1, c->stream));
-    CK(launch_to_float(c->d_tab64, c->d_tab32, c->tab_pad_total, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
   c->have_proj = true;
@@ -994,7 +990,6 @@ static int ensure_dtab(sqb_ctx *c) {
   p.typ_size = c->d_typ_size;
   p.typ_tab = c->d_typ_tab;
   p.tables = c->d_tables;
-  p.out32 = nullptr;
   p.total = c->tab_total;
   p.status = c->d_status;
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));

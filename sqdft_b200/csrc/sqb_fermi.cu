@@ -289,7 +289,6 @@ __global__ void proj_kernel(ProjArgs a) {
     const double u = UlJ * real_sh(xr, yr, zr, rad, l, m) * (VlJ - VlocJ);
     const long long o = a.rep_off[r] + ((long long)q * Sd + ctr / (Sd * Sd)) * plane_stride(Sd) + ctr % (Sd * Sd);
     a.out64[o] = u;
-    if (a.out32) a.out32[o] = (float)u;
   }
 }
 
@@ -340,11 +339,6 @@ __global__ void repack_kernel(const int *rep_nn, const int *typ_nlocc, const int
 __global__ void fd_combine_kernel(const double *plus, const double *minus, double *out, long long n, double scale) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     out[i] = (plus[i] - minus[i]) * scale;
-}
-
-__global__ void to_float_kernel(const double *in, float *out, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    out[i] = (float)in[i];
 }
 
 size_t fermi_smem(int K, int per_warp, bool &fits) {
@@ -399,12 +393,6 @@ cudaError_t launch_projectors(const ProjArgs &a, cudaStream_t s) {
 
 cudaError_t launch_minmax(const double *lmin, const double *lmax, int n, double *out, cudaStream_t s) {
   minmax_kernel<<<1, 1024, 0, s>>>(lmin, lmax, n, out);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_to_float(const double *in, float *out, long long n, cudaStream_t s) {
-  if (n <= 0) return cudaSuccess;
-  to_float_kernel<<<296, 256, 0, s>>>(in, out, n);
   return cudaGetLastError();
 }
 

@@ -42,7 +42,6 @@ struct DevAtoms {
   const int *typ_nproj;     // [n_typ]
   const double *proj_denom; // [n_typ][MAXPROJ_TYPE]
   const double *tab64;      // projector tables, padded planes, FP64
-  const float *tab32;       // the same in FP32 (mixed path)
 };
 
 enum NodeMode : int { MODE_SQ = 0, MODE_FORCES = 1, MODE_APPLY = 2, MODE_MOMENTS = 3, MODE_VJP = 4 };
@@ -62,7 +61,6 @@ struct NodeArgs {
   double coeff_lap[FDN + 1];
   double coeff_grad[FDN + 1];
   const double *veff64;
-  const float *veff32;
   DevAtoms at;
   const int *node_list; // nodes to process
   int n_list;
@@ -105,7 +103,9 @@ cudaError_t launch_node_kernel(const NodeArgs &a, int grid, int cols, cudaStream
 cudaError_t setup_node_forces(int n);
 cudaError_t launch_node_forces(const NodeArgs &a, int grid, int cols, cudaStream_t s);
 cudaError_t setup_node_vjp(int n);
+cudaError_t setup_node_sq32(int n);
 cudaError_t launch_node_vjp(const NodeArgs &a, int grid, int cols, cudaStream_t s);
+cudaError_t launch_node_sq32(const NodeArgs &a, int grid, int cols, cudaStream_t s);
 cudaError_t node_kernel_setup(int n);
 // Stage size wanted for a per-plane footprint of `elems` values (the launcher
 // clamps it to what the launch's shared memory leaves).
@@ -142,12 +142,10 @@ struct ProjArgs {
   const long long *typ_tab; // offset of each type's 19 x size tables
   const double *tables;
   double *out64;
-  float *out32;  // may be NULL (no FP32 copy)
   long long total;
   int *status;
 };
 cudaError_t launch_projectors(const ProjArgs &a, cudaStream_t s);
-cudaError_t launch_to_float(const double *in, float *out, long long n, cudaStream_t s);
 // out = (plus - minus) * scale, element-wise.
 cudaError_t launch_fd_combine(const double *plus, const double *minus, double *out, long long n, double scale,
                               cudaStream_t s);

@@ -32,6 +32,7 @@
 // warp's rows (the same list for every lane), each lane testing its column.
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 
 #include "sqb_internal.cuh"
 
@@ -41,7 +42,7 @@ namespace sqb {
 // node_kernel_setup.
 extern int g_smem_optin;
 
-enum : int { KIND_SQ = 0, KIND_FORCES = 1, KIND_VJP = 2 };
+enum : int { KIND_SQ = 0, KIND_FORCES = 1, KIND_VJP = 2, KIND_SQ32 = 3 };
 
 namespace {
 
@@ -120,18 +121,6 @@ struct PassIO {
   long long dstride = 0;
 };
 
-template <typename T>
-__device__ __forceinline__ const T *veff_of(const NodeArgs &a);
-template <>
-__device__ __forceinline__ const double *veff_of<double>(const NodeArgs &a) { return a.veff64; }
-template <>
-__device__ __forceinline__ const float *veff_of<float>(const NodeArgs &a) { return a.veff32; }
-template <typename T>
-__device__ __forceinline__ const T *tab_of(const NodeArgs &a);
-template <>
-__device__ __forceinline__ const double *tab_of<double>(const NodeArgs &a) { return a.at.tab64; }
-template <>
-__device__ __forceinline__ const float *tab_of<float>(const NodeArgs &a) { return a.at.tab32; }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -237,7 +226,6 @@ __device__ __forceinline__ void arm_plane(NodeShared &S, int zz, int st, size_t 
 
 // Issue the bulk copies of plane zz's table planes into stage st, spread
 // over the warps: the k-th box crossing the plane goes to warp k % nw.
-template <typename T>
 __device__ void issue_plane(const NodeArgs &a, NodeShared &S, unsigned char *dyn, int zz, int st) {
   const int nw = blockDim.x >> 5;
   const int k = (threadIdx.x & 31) * nw + (threadIdx.x >> 5);
@@ -245,14 +233,14 @@ __device__ void issue_plane(const NodeArgs &a, NodeShared &S, unsigned char *dyn
   const int e = cross_list(a, dyn)[zz * MAXE + k];
   const int off = off_table(a, dyn)[zz * MAXE + e];
   if (off < 0) return;
-  T *stage = stage_ptr<T>(a, dyn, st);
-  const T *tab = tab_of<T>(a);
+  double *stage = stage_ptr<double>(a, dyn, st);
+  const double *tab = a.at.tab64;
   const int Sd = S.e_S[e], sp2 = S.e_sp2[e], cnt = S.e_sc[e];
-  const T *src = tab + S.e_tab[e] + (long long)(S.e_tz0[e] + zz) * sp2 + S.e_ss[e];
+  const double *src = tab + S.e_tab[e] + (long long)(S.e_tz0[e] + zz) * sp2 + S.e_ss[e];
   // No proxy fence: every generic-proxy read of this stage (plane zz-3) was
   // consumed before the barrier that precedes this call.
   for (int q = 0; q < S.e_np[e]; q++)
-    bulk_g2s(stage + off + q * cnt, src + (long long)q * Sd * sp2, (unsigned)(cnt * sizeof(T)), &S.mbar[st]);
+    bulk_g2s(stage + off + q * cnt, src + (long long)q * Sd * sp2, (unsigned)(cnt * sizeof(double)), &S.mbar[st]);
 }
 
 // Wait for the copies of a stage (every thread); a wait that runs out of time
@@ -344,19 +332,20 @@ __device__ void block_sum3(NodeShared &S, double v0, double v1, double v2) {
 // plane zz (the k-th crossing box goes to warp k % nw); the table planes come
 // from the plane's stage, or from global memory for a box that was not staged.
 template <typename T>
-__device__ __forceinline__ double box_dot(const T *pl, int pitch, const T *U, int Sd, int bx, int by, int lane) {
+__device__ __forceinline__ double box_dot(const T *pl, int pitch, const double *U, int Sd, int bx, int by, int lane) {
   double acc = 0.0;
   if (bx <= 16) {  // two rows per step: lanes 0-15 and 16-31
     const int lr = lane >> 4, lx = lane & 15;
     if (lx < bx) {
-      const T *p = pl + lr * pitch + lx, *u = U + lr * Sd + lx;
-      for (int y = lr; y < by; y += 2, p += 2 * pitch, u += 2 * Sd) acc += (double)*p * (double)*u;
+      const T *p = pl + lr * pitch + lx;
+      const double *u = U + lr * Sd + lx;
+      for (int y = lr; y < by; y += 2, p += 2 * pitch, u += 2 * Sd) acc += (double)*p * *u;
     }
   } else {
     const RowLanes L(bx, lane);
     if (L.lr < L.R) {
       for (int y = L.lr; y < by; y += L.R)
-        for (int x = L.lx; x < bx; x += L.W) acc += (double)pl[y * pitch + x] * (double)U[y * Sd + x];
+        for (int x = L.lx; x < bx; x += L.W) acc += (double)pl[y * pitch + x] * U[y * Sd + x];
     }
   }
   return acc;
@@ -377,8 +366,8 @@ __device__ __forceinline__ double box_dot_d(const T *pl, int pitch, const double
 // derivative tables dchi/dR_alpha of every crossing box, added to pg[alpha][p]
 // (read from global memory: this runs only in the adjoint kernel group).
 template <typename T>
-__device__ void dot_phase(NodeShared &S, const T *plane, int zz, int pitch, const T *tab, const short *offz,
-                          const unsigned char *crossz, const T *stage, double *pg = nullptr,
+__device__ void dot_phase(NodeShared &S, const T *plane, int zz, int pitch, const double *tab, const short *offz,
+                          const unsigned char *crossz, const double *stage, double *pg = nullptr,
                           const double *dtab = nullptr, long long dstride = 0) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int k = warp; k < S.ncross[zz]; k += nw) {
@@ -450,8 +439,8 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
   const int centre_col = a.nloc * n + a.nloc;
   T *sm_in = reinterpret_cast<T *>(dyn);
   T *sm_out = sm_in + 2 * P2;
-  const T *veff = veff_of<T>(a);
-  const T *tab = tab_of<T>(a);
+  const double *veff = a.veff64;  // Veff and projector tables stay FP64 in both paths
+  const double *tab = a.at.tab64;
   const size_t vplane = (size_t)a.ex * a.ey;
   const short *off_tab = off_table(a, dyn);
   const bool staged = (STENCIL || DOTS) && S.n_ent > 0;
@@ -459,10 +448,10 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
   if (STENCIL) {
     for (int i = tid; i < 2 * P2; i += nt) sm_in[i] = T(0);
   }
-  if (staged && tid == 0) arm_plane(S, 0, 0, sizeof(T));
+  if (staged && tid == 0) arm_plane(S, 0, 0, sizeof(double));
   __syncthreads();
   int ph = S.ph;
-  if (staged) issue_plane<T>(a, S, dyn, 0, 0);
+  if (staged) issue_plane(a, S, dyn, 0, 0);
 
   int col[C], cx[C], cy[C];
   bool ok[C];
@@ -497,7 +486,8 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
     if (!ok[c] || z >= n) return T(0);
     return form_w<T>(io, (size_t)z * n2 + col[c], pf[c], rw1[c], rw2[c]);
   };
-  T q_ve[C], q_p1[C], q_p2[C];
+  T q_p1[C], q_p2[C];
+  double q_ve[C];
   double q_d[C];
   auto ld_point = [&](int c, int z) {
     if (!ok[c] || z >= n) return;
@@ -568,12 +558,12 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
     }
     const int st_next = st == NSTAGE - 1 ? 0 : st + 1, st_prev = st == 0 ? NSTAGE - 1 : st - 1;
     if (staged && z < n) stage_wait(a, S, st, ph);
-    if (staged && tid == 0 && z + 1 < n) arm_plane(S, z + 1, st_next, sizeof(T));
+    if (staged && tid == 0 && z + 1 < n) arm_plane(S, z + 1, st_next, sizeof(double));
     __syncthreads();
     if (DOTS && z >= 1 && S.n_ent > 0)
       dot_phase<T>(S, sm_out + ((z - 1) & 1) * n2, z - 1, n, tab, off_tab + (z - 1) * MAXE,
-                   cross_list(a, dyn) + (z - 1) * MAXE, stage_ptr<T>(a, dyn, st_prev), io.pg, io.dtab, io.dstride);
-    if (staged && z + 1 < n) issue_plane<T>(a, S, dyn, z + 1, st_next);
+                   cross_list(a, dyn) + (z - 1) * MAXE, stage_ptr<double>(a, dyn, st_prev), io.pg, io.dtab, io.dstride);
+    if (staged && z + 1 < n) issue_plane(a, S, dyn, z + 1, st_next);
     if (z == n) break;
     // Nonlocal gather: the boxes covering this warp's rows and crossing plane
     // z, the same list for every lane; each lane adds the boxes that cover
@@ -583,7 +573,7 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
     for (int c = 0; c < C; c++) vnl[c] = 0.0;
     if (STENCIL && S.n_ent > 0) {
       const short *offz = off_tab + z * MAXE;
-      const T *stg = stage_ptr<T>(a, dyn, st);
+      const double *stg = stage_ptr<double>(a, dyn, st);
 #pragma unroll
       for (int w = 0; w < 4; w++) {
         uint32_t m = wmask[w] & S.zmask[z][w];
@@ -596,21 +586,21 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
           const int tx0 = (short)(g.y & 0xffff), ty0 = g.y >> 16;
           const int Sd = g.z & 0xff, np = (g.z >> 8) & 0xff, pb = g.z >> 16, ss = g.w & 0xffff, cnt = g.w >> 16;
           if (off >= 0) {  // shared-memory stage: its own pointer, so the loads stay shared loads
-            const T *base = stg + off - ss;
+            const double *base = stg + off - ss;
 #pragma unroll
             for (int c = 0; c < C; c++) {
               if (!ok[c] || cx[c] < x0 || cx[c] > x1 || cy[c] < y0 || cy[c] > y1) continue;
-              const T *u = base + (ty0 + cy[c]) * Sd + tx0 + cx[c];
-              for (int q = 0; q < np; q++) vnl[c] += S.p_cur[pb + q] * (double)u[q * cnt];
+              const double *u = base + (ty0 + cy[c]) * Sd + tx0 + cx[c];
+              for (int q = 0; q < np; q++) vnl[c] += S.p_cur[pb + q] * u[q * cnt];
             }
           } else {
             const int sp2 = S.e_sp2[e];
-            const T *base = tab + S.e_tab[e] + (long long)(S.e_tz0[e] + z) * sp2;
+            const double *base = tab + S.e_tab[e] + (long long)(S.e_tz0[e] + z) * sp2;
 #pragma unroll
             for (int c = 0; c < C; c++) {
               if (!ok[c] || cx[c] < x0 || cx[c] > x1 || cy[c] < y0 || cy[c] > y1) continue;
-              const T *u = base + (ty0 + cy[c]) * Sd + tx0 + cx[c];
-              for (int q = 0; q < np; q++) vnl[c] += S.p_cur[pb + q] * (double)u[(long long)q * Sd * sp2];
+              const double *u = base + (ty0 + cy[c]) * Sd + tx0 + cx[c];
+              for (int q = 0; q < np; q++) vnl[c] += S.p_cur[pb + q] * u[(long long)q * Sd * sp2];
             }
           }
         }
@@ -630,7 +620,7 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
           T s = smz[idx - k] + smz[idx + k] + smz[idx - k * P] + smz[idx + k * P] + win[c][FDN - k] + win[c][FDN + k];
           temp += (double)s * a.coeff_lap[k];
         }
-        hv = -0.5 * temp + (double)q_ve[c] * v + vnl[c];
+        hv = -0.5 * temp + q_ve[c] * v + vnl[c];
       }
       T o = T(0);
       if constexpr (PK == PK_ONES) {
@@ -728,8 +718,8 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
   const int x = lane;
   T *sm_in = reinterpret_cast<T *>(dyn);
   T *sm_out = sm_in + 2 * RPLANE;
-  const T *veff = veff_of<T>(a);
-  const T *tab = tab_of<T>(a);
+  const double *veff = a.veff64;  // Veff and projector tables stay FP64 in both paths
+  const double *tab = a.at.tab64;
   const size_t vplane = (size_t)a.ex * a.ey;
   const short *off_tab = off_table(a, dyn);
   const bool staged = (STENCIL || DOTS) && S.n_ent > 0;
@@ -737,10 +727,10 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
   if (STENCIL) {
     for (int i = tid; i < 2 * RPLANE; i += nt) sm_in[i] = T(0);
   }
-  if (staged && tid == 0) arm_plane(S, 0, 0, sizeof(T));
+  if (staged && tid == 0) arm_plane(S, 0, 0, sizeof(double));
   __syncthreads();
   int ph = S.ph;
-  if (staged) issue_plane<T>(a, S, dyn, 0, 0);
+  if (staged) issue_plane(a, S, dyn, 0, 0);
 
   int y[RY];
   bool ok[RY];
@@ -760,7 +750,8 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
     else return io.vin[(size_t)z * n2 + col[j]] * sin;
   };
   T win[RY][2 * FDN + 1];
-  T pf[RY], q_ve[RY], q_p1[RY], q_p2[RY];
+  T pf[RY], q_p1[RY], q_p2[RY];
+  double q_ve[RY];
   T rw1[RY], rw2[RY];  // PK_LZF: W1, W2 of the prefetched plane (pf holds its Y)
   auto lzf_load = [&](int j, int z) {
     if (ok[j] && z < n && !io.konst) {
@@ -832,12 +823,12 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
     }
     const int st_next = st == NSTAGE - 1 ? 0 : st + 1, st_prev = st == 0 ? NSTAGE - 1 : st - 1;
     if (staged && z < n) stage_wait(a, S, st, ph);
-    if (staged && tid == 0 && z + 1 < n) arm_plane(S, z + 1, st_next, sizeof(T));
+    if (staged && tid == 0 && z + 1 < n) arm_plane(S, z + 1, st_next, sizeof(double));
     __syncthreads();
     if (DOTS && z >= 1 && S.n_ent > 0)
       dot_phase<T>(S, sm_out + ((z - 1) & 1) * OPLANE, z - 1, 32, tab, off_tab + (z - 1) * MAXE,
-                   cross_list(a, dyn) + (z - 1) * MAXE, stage_ptr<T>(a, dyn, st_prev), io.pg, io.dtab, io.dstride);
-    if (staged && z + 1 < n) issue_plane<T>(a, S, dyn, z + 1, st_next);
+                   cross_list(a, dyn) + (z - 1) * MAXE, stage_ptr<double>(a, dyn, st_prev), io.pg, io.dtab, io.dstride);
+    if (staged && z + 1 < n) issue_plane(a, S, dyn, z + 1, st_next);
     if (z == n) break;
 
     double vnl[RY];
@@ -845,7 +836,7 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
     for (int j = 0; j < RY; j++) vnl[j] = 0.0;
     if (STENCIL && S.n_ent > 0) {
       const short *offz = off_tab + z * MAXE;
-      const T *stg = stage_ptr<T>(a, dyn, st);
+      const double *stg = stage_ptr<double>(a, dyn, st);
       if constexpr (RY == 2) {
         // the boxes of this warp's item list that cross plane z
         const int4 *it = row_items(a, dyn) + warp * ITEMS;
@@ -859,7 +850,7 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
           const int pb = g.w & 0xffff, cnt = g.w >> 16;
           const int off = offz[e];
           if (off >= 0) {  // shared-memory stage: its own pointer, so the loads stay shared loads
-            const T *u = stg + off + rb;
+            const double *u = stg + off + rb;
             for (int q = 0; q < np; q++) {
               const double pc = S.p_cur[pb + q];
               if (fl & 1) vnl[0] += pc * (double)u[q * cnt];
@@ -867,7 +858,7 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
             }
           } else {
             const int sp2 = S.e_sp2[e];
-            const T *u = tab + S.e_tab[e] + (long long)(S.e_tz0[e] + z) * sp2 + rb + S.e_ss[e];
+            const double *u = tab + S.e_tab[e] + (long long)(S.e_tz0[e] + z) * sp2 + rb + S.e_ss[e];
             for (int q = 0; q < np; q++) {
               const double pc = S.p_cur[pb + q];
               if (fl & 1) vnl[0] += pc * (double)u[(long long)q * Sd * sp2];
@@ -890,20 +881,20 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
           const int tx0 = (short)(g.y & 0xffff), ty0 = g.y >> 16;
           const int Sd = g.z & 0xff, np = (g.z >> 8) & 0xff, pb = g.z >> 16, ss = g.w & 0xffff, cnt = g.w >> 16;
           if (off >= 0) {
-            const T *base = stg + off - ss + tx0 + x;
+            const double *base = stg + off - ss + tx0 + x;
 #pragma unroll
             for (int j = 0; j < RY; j++) {
               if (!ok[j] || y[j] < y0 || y[j] > y1) continue;
-              const T *u = base + (ty0 + y[j]) * Sd;
+              const double *u = base + (ty0 + y[j]) * Sd;
               for (int q = 0; q < np; q++) vnl[j] += S.p_cur[pb + q] * (double)u[q * cnt];
             }
           } else {
             const int sp2 = S.e_sp2[e];
-            const T *base = tab + S.e_tab[e] + (long long)(S.e_tz0[e] + z) * sp2 + tx0 + x;
+            const double *base = tab + S.e_tab[e] + (long long)(S.e_tz0[e] + z) * sp2 + tx0 + x;
 #pragma unroll
             for (int j = 0; j < RY; j++) {
               if (!ok[j] || y[j] < y0 || y[j] > y1) continue;
-              const T *u = base + (ty0 + y[j]) * Sd;
+              const double *u = base + (ty0 + y[j]) * Sd;
               for (int q = 0; q < np; q++) vnl[j] += S.p_cur[pb + q] * (double)u[(long long)q * Sd * sp2];
             }
           }
@@ -950,7 +941,7 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
 #pragma unroll
       for (int j = 0; j < RY; j++) {
         vj[j] = (double)win[j][FDN];
-        hvj[j] = -0.5 * temp[j] + (double)q_ve[j] * vj[j] + vnl[j];
+        hvj[j] = -0.5 * temp[j] + q_ve[j] * vj[j] + vnl[j];
       }
     }
 
@@ -1308,7 +1299,8 @@ __device__ void count_proj_points(const NodeArgs &a, NodeShared &S, int passes, 
   if (cheb) atomicAdd(a.proj_points + 1, s * (unsigned long long)passes);
 }
 
-// Lanczos bounds (FP64), sq.cpp:965-1092, one sweep per Lanczos step.
+// Lanczos bounds, sq.cpp:965-1092, one sweep per Lanczos step; vectors stored
+// in T (FP32 in the mixed path), recurrences, dots and T_m in FP64.
 //
 // The reference's step k computes u = H v_k+1, a = <v_k+1, u>, w = u - a v_k+1
 // - b v_k, b' = |w|, v_k+2 = w / b'.  Here sweep m applies H to the
@@ -1321,18 +1313,18 @@ __device__ void count_proj_points(const NodeArgs &a, NodeShared &S, int passes, 
 // from the same recurrence on the projections: chi^T W_m+1 = s_m (chi^T Y_m -
 // a_m chi^T W_m) - b_m-1 s_m-1 chi^T W_m-1, with chi^T Y_m the dot products
 // of the sweep's output.  The matvec count is the reference's (count + 1).
-template <int C>
+template <typename T, int C>
 __device__ void lanczos(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const uint32_t (&mask)[4],
                         double &lmin_out, double &lmax_out, int &iters) {
   const double nw = (double)a.n * a.n * a.n;
-  double *Y = slot<double>(a, 0);
-  double *W[2] = {slot<double>(a, 1), slot<double>(a, 2)};
+  T *Y = slot<T>(a, 0);
+  T *W[2] = {slot<T>(a, 1), slot<T>(a, 2)};
   double d0 = 0.0, d1 = 0.0;
   // chi^T W_0 with W_0 = v_0 = ones / |ones| (sq.cpp:538-546, 993-1004)
   {
-    PassIO<double> io;
+    PassIO<T> io;
     io.out = W[1];  // scratch: W[1] is overwritten before it is read
-    run_pass<double, C, PK_ONES>(a, S, dyn, io, mask, d0, d1);
+    run_pass<T, C, PK_ONES>(a, S, dyn, io, mask, d0, d1);
     const double s0 = 1.0 / sqrt(nw);
     for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) {
       S.pw_cur[p] = s0 * S.p_nxt[p];
@@ -1351,7 +1343,7 @@ __device__ void lanczos(const NodeArgs &a, NodeShared &S, unsigned char *dyn, co
   }
   __syncthreads();
   for (int m = 0;; m++) {
-    PassIO<double> io;
+    PassIO<T> io;
     io.out = Y;
     io.wout = W[m & 1];
     if (m == 0) {
@@ -1367,7 +1359,7 @@ __device__ void lanczos(const NodeArgs &a, NodeShared &S, unsigned char *dyn, co
     }
     d0 = 0.0;
     d1 = 0.0;
-    run_pass<double, C, PK_LZF>(a, S, dyn, io, mask, d0, d1);
+    run_pass<T, C, PK_LZF>(a, S, dyn, io, mask, d0, d1);
     block_sum3(S, d0, d1, 0.0);
     // b_m-1 = |W_m| and a_m = <W_m, H W_m> / b_m-1^2 (W_0 is normalised)
     const double bm = m == 0 ? 1.0 : sqrt(S.scal[0]);
@@ -1811,8 +1803,9 @@ __device__ void node_vjp(const NodeArgs &a, NodeShared &S, unsigned char *dyn, c
 // L is the plane-loop layout (L > 0: L columns per thread; L < 0: -L rows
 // per warp); MAXT is the launch bound, which sets the register budget per
 // thread (64K / MAXT); KIND selects the modes the instantiation carries
-// (KIND_SQ: SQ, moments with given bounds, matvec; KIND_FORCES; KIND_VJP),
-// so the register allocation of each is its own.
+// (KIND_SQ: SQ, moments with given bounds, matvec; KIND_SQ32: SQ of the
+// FP32-mixed path, Lanczos vectors in FP32; KIND_FORCES; KIND_VJP), so the
+// register allocation of each is its own.
 template <int C, int MAXT, int KIND>
 __global__ void __launch_bounds__(MAXT, 1) node_kernel(NodeArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1848,13 +1841,14 @@ __global__ void __launch_bounds__(MAXT, 1) node_kernel(NodeArgs a) {
       build_items(a, S, row_items(a, dyn));
       __syncthreads();
     }
-    if constexpr (KIND == KIND_SQ) {
+    if constexpr (KIND == KIND_SQ || KIND == KIND_SQ32) {
+      using TV = typename std::conditional<KIND == KIND_SQ32, float, double>::type;
       if (a.mode == MODE_SQ || a.mode == MODE_MOMENTS) {
         // SQ: Lanczos bounds then moments; MODE_MOMENTS: moments with given bounds
         double lmin = 0.0, lmax = 0.0, chi, zee;
         int iters = 0;
         if (a.mode == MODE_SQ) {
-          lanczos<C>(a, S, dyn, mask, lmin, lmax, iters);
+          lanczos<TV, C>(a, S, dyn, mask, lmin, lmax, iters);
           chi = (lmax + lmin) / 2;  // sq.cpp:564-565
           zee = (lmax - lmin) / 2;
         } else {
@@ -1862,8 +1856,10 @@ __global__ void __launch_bounds__(MAXT, 1) node_kernel(NodeArgs a) {
           zee = a.zee_in[node];
         }
         double *mu = a.rho_pj + (size_t)node * (a.npl + 1);
-        if (a.mixed) moments<float, C>(a, S, dyn, mask, chi, zee, mu);
-        else moments<double, C>(a, S, dyn, mask, chi, zee, mu);
+        // moments stay FP64 in both paths: FP32 storage of the Chebyshev
+        // vectors grows a rounding error injected at step i like (k - i) by
+        // step k, ~5e-6 of max rho after 48 steps, above the mixed budget
+        moments<double, C>(a, S, dyn, mask, chi, zee, mu);
         if (a.mode == MODE_SQ && threadIdx.x == 0) {
           a.chi[node] = chi;
           a.zee[node] = zee;
@@ -1871,7 +1867,7 @@ __global__ void __launch_bounds__(MAXT, 1) node_kernel(NodeArgs a) {
           if (a.lmax) a.lmax[node] = lmax;
           if (a.lanczos_iters) a.lanczos_iters[node] = iters;
         }
-      } else {
+      } else if constexpr (KIND == KIND_SQ) {
         const size_t nw = (size_t)a.n * a.n * a.n;
         double d0 = 0.0, d1 = 0.0;
         PassIO<double> io;

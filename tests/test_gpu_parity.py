@@ -7,10 +7,11 @@ Tolerances (FP64 path vs the reference FP64 path):
   rho                     |d rho|_inf <= 1e-10
   Ebs, Eent per atom      1e-8 Ha/atom
   nonlocal forces         1e-7 Ha/bohr
-FP32-mixed path vs the reference FP64 outputs: max-norm rho error relative
-to max rho <= 1e-5 (measured 1.2e-6 on tiny, 5.6e-6 on the 4,096-node Al
-cell; the 1e-6 target of the mixed path is not met), Ebs/Eent <= 1e-6 Ha/atom,
-forces <= 1e-4 Ha/bohr.
+FP32-mixed path (FP32 Lanczos vectors, FP64 moments) vs the reference FP64
+outputs: max-norm rho error relative to max rho <= 1e-6, Ebs/Eent <= 1e-6
+Ha/atom (the FP32 Lanczos moves the bounds, hence the Chebyshev truncation,
+by ~1e-7 Ha), forces <= 1e-6 Ha/bohr; with the looser Lanczos stop of 1e-3 Ha on
+the 110,592-node Al cell (npl 96) rho <= 1e-6 against the FP64 path.
 """
 from __future__ import annotations
 
@@ -97,17 +98,42 @@ def test_lanczos_iterations_match_oracle(golden):
     assert np.abs(m["lmax"] - orc["lmax"]).max() <= 1e-10
 
 
-@pytest.mark.parametrize("name", ["tiny", "mid"])
+@pytest.mark.parametrize("name", ["tiny", "lihs", "mid"])
 def test_mixed_precision_budget(golden, name):
     case, ref = golden(name)
     with _ctx(case, precision=1) as ctx:
         out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
         f = ctx.forces_nonlocal()
     rel = np.abs(out["rho"] - ref["rho"]).max() / np.abs(ref["rho"]).max()
-    assert rel <= 1e-5, rel
-    assert abs(out["Ebs"] - ref["Ebs"][0]) / case.n_atm <= 1e-6
-    assert abs(out["Eent"] - ref["Eent"][0]) / case.n_atm <= 1e-6
-    assert np.abs(f - ref["fnloc"]).max() <= 1e-4
+    ebs = abs(out["Ebs"] - ref["Ebs"][0]) / case.n_atm
+    eent = abs(out["Eent"] - ref["Eent"][0]) / case.n_atm
+    print(f"mixed {name}: rho {rel:.2e} lambda {abs(out['lambda_f'] - ref['lambda_f'][0]):.1e} "
+          f"Ebs {ebs:.1e} Eent {eent:.1e} Ha/atom F {np.abs(f - ref['fnloc']).max():.1e}")
+    assert rel <= 1e-6, rel
+    assert ebs <= 1e-6 and eent <= 1e-6
+    assert np.abs(f - ref["fnloc"]).max() <= 1e-6
+
+
+def test_mixed_loose_lanczos_budget():
+    """The 110,592-node Al cell (31^3 windows, npl 96): with the Lanczos stop
+    at 1e-3 Ha the mixed path takes ~35 instead of 64 Lanczos steps per node
+    and its density stays within 1e-6 of max rho of the FP64 path's."""
+    from sqdft_b200 import sq
+    from sqdft_b200.cases import load
+
+    case = load("c2")
+    outs, iters = [], []
+    for prec in (0, 1):
+        with sq.Context(case, device=0, precision=prec) as ctx:
+            ctx.set_mixed_lanczos_tol(1e-3)
+            ctx.nonlocal_projectors()
+            outs.append(ctx.spectral_quadrature(case.scf_iter, case.lambda_f))
+            iters.append(ctx.stats()["lanczos_iters"])
+    rel = np.abs(outs[1]["rho"] - outs[0]["rho"]).max() / np.abs(outs[0]["rho"]).max()
+    print(f"mixed c2 (Lanczos stop 1e-3): rho {rel:.2e}, Lanczos steps {iters[1] / iters[0]:.2f} of FP64")
+    assert rel <= 1e-6
+    assert iters[1] <= 0.65 * iters[0]
+    assert abs(outs[1]["Ebs"] - outs[0]["Ebs"]) / case.n_atm <= 1e-6
 
 
 def test_deterministic(golden):
