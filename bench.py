@@ -15,8 +15,8 @@ e2e    nodes / (wall time of the C-ABI call with host buffers: Veff copied
        in from pinned memory, rho, rho_pj, Ci, chi, zee copied out)
 With N > 1 (torchrun, NCCL), rank r owns a z-slab of the grid; the
 Fermi-level sums and energies are all-reduced through the library's hook.
---precision mixed runs the FP32-mixed path (FP32 Lanczos vectors with the
-Lanczos stop at T Ha, FP64 moments) and, outside the timed region, one FP64
+--precision mixed runs the FP32-mixed path (FP32 Lanczos vectors from a
+checkerboard-weighted start, stopping at T Ha; FP64 moments) and, outside the timed region, one FP64
 step of the same input to state the density error against it.
 --impl reference times the reference SQDFT compiled from its sources
 (oracle/_ref/sqref_driver: its LanczosAlgorithm and HsubTimesVec per node)
@@ -134,7 +134,7 @@ def run_ours(args):
 
     ctx = sq.Context(my, device=local, precision=prec, allreduce=allreduce_fn(dist, "cuda") if ws > 1 else None)
     if prec == sq.SQB_FP32_MIXED:
-        ctx.set_mixed_lanczos_tol(args.mixed_lanczos_tol)
+        ctx.set_mixed_lanczos(args.mixed_lanczos_tol)
     ctx.nonlocal_projectors()
     n = my.n_nodes
     K1 = my.npl + 1

@@ -26,6 +26,7 @@ struct sqb_ctx {
   cudaStream_t stream = nullptr;
   int precision = SQB_FP64;
   double mixed_lanczos_tol = 0.0;  // Ha: the mixed path's Lanczos stop and margin (0: the grid's)
+  double mixed_lanczos_chk = 0.5;  // checkerboard weight of the mixed path's Lanczos start vector
   int cols = 0, ctas_per_sm = 1;
   int use_graph = 0;                       // replay the node-kernel sequence from a CUDA graph
   cudaGraphExec_t sq_graph = nullptr;      // captured Lanczos+moments sequence (node kernel, min/max)
@@ -159,6 +160,7 @@ void fill_node_args(sqb_ctx *c, NodeArgs &a) {
   a.h3 = c->h3;
   a.mixed = c->precision == SQB_FP32_MIXED;
   a.lanczos_tol = a.mixed ? std::max(c->g.lanczos_tol, c->mixed_lanczos_tol) : c->g.lanczos_tol;
+  a.lz_chk = a.mixed ? c->mixed_lanczos_chk : 0.0;
   for (int k = 0; k <= FDN; k++) {
     a.coeff_lap[k] = c->g.coeff_lap[k];
     a.coeff_grad[k] = c->g.coeff_grad[k];
@@ -481,9 +483,10 @@ int sqb_set_precision(sqb_ctx *c, int precision) {
   return SQB_OK;
 }
 
-int sqb_set_mixed_lanczos_tol(sqb_ctx *c, double tol) {
-  if (!c || !(tol >= 0.0) || !std::isfinite(tol)) return SQB_ERR_ARG;
+int sqb_set_mixed_lanczos(sqb_ctx *c, double tol, double checkerboard) {
+  if (!c || !(tol >= 0.0) || !std::isfinite(tol) || !(checkerboard >= 0.0 && checkerboard <= 1.0)) return SQB_ERR_ARG;
   c->mixed_lanczos_tol = tol;
+  c->mixed_lanczos_chk = checkerboard;
   drop_graph(c);
   return SQB_OK;
 }

@@ -58,6 +58,7 @@ struct NodeArgs {
   int npl;
   double h3;     // pow(delta, 3)
   double lanczos_tol;
+  double lz_chk;      // checkerboard weight of the Lanczos start vector (0: the reference's ones)
   double coeff_lap[FDN + 1];
   double coeff_grad[FDN + 1];
   const double *veff64;

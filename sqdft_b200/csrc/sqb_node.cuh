@@ -115,7 +115,8 @@ struct PassIO {
   double cd = 0.0, ce = 0.0;    // D coefficients (forces)
   int dbl = 0;                  // accumulate the doubling dot products
   T *wout = nullptr;            // PK_LZF: where the formed input is stored
-  int konst = 0;                // PK_LZF: the input is the constant sin
+  int konst = 0;                // PK_LZF: the input is sin times the start vector
+  double chk = 0.0;             // start vector 1 + chk (-1)^(x+y+z) (PK_ONES, PK_LZF konst)
   double *pg = nullptr;         // adjoint with atom gradients: dots with dchi/dR_alpha, [3][MAXP]
   const double *dtab = nullptr; // dchi/dR tables (3 x stride values)
   long long dstride = 0;
@@ -419,9 +420,14 @@ __device__ void rotate_proj(NodeShared &S, double scale) {
 // v_k = s1 W1, v_k-1 = s2 W2 and cb = b s2 (LanczosAlgorithm, sq.cpp:1032-1036);
 // stored in wout, in place of W2.  The operands are loaded one plane before
 // they are combined, so the loads' latency overlaps a plane of work.
+// Lanczos start vector at window index g: 1 + chk (-1)^(x+y+z); the window
+// edge n is odd, so x + y + z and g = (z n + y) n + x have the same parity.
+__device__ __forceinline__ double start_val(double chk, size_t g) { return 1.0 + chk * (1.0 - 2.0 * (double)(g & 1)); }
+
 template <typename T>
 __device__ __forceinline__ T form_w(const PassIO<T> &io, size_t g, T y, T w1, T w2) {
-  const T f = io.konst ? (T)io.sin : (T)(io.s1 * ((double)y - io.ca * (double)w1) - io.cb * (double)w2);
+  const T f = io.konst ? (T)(io.sin * start_val(io.chk, g))
+                       : (T)(io.s1 * ((double)y - io.ca * (double)w1) - io.cb * (double)w2);
   io.wout[g] = f;
   return f;
 }
@@ -624,7 +630,7 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
       }
       T o = T(0);
       if constexpr (PK == PK_ONES) {
-        o = T(1);
+        o = (T)start_val(io.chk, g);
         io.out[g] = o;
       } else if constexpr (PK == PK_DELTA) {
         o = (col[c] == centre_col && z == a.nloc) ? T(1) : T(0);
@@ -952,7 +958,7 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
       const double hv = STENCIL ? hvj[j] : 0.0, v = STENCIL ? vj[j] : 0.0;
       T o = T(0);
       if constexpr (PK == PK_ONES) {
-        o = T(1);
+        o = (T)start_val(io.chk, g);
         io.out[g] = o;
       } else if constexpr (PK == PK_DELTA) {
         o = (x == a.nloc && y[j] == a.nloc && z == a.nloc) ? T(1) : T(0);
@@ -1320,12 +1326,17 @@ __device__ void lanczos(const NodeArgs &a, NodeShared &S, unsigned char *dyn, co
   T *Y = slot<T>(a, 0);
   T *W[2] = {slot<T>(a, 1), slot<T>(a, 2)};
   double d0 = 0.0, d1 = 0.0;
-  // chi^T W_0 with W_0 = v_0 = ones / |ones| (sq.cpp:538-546, 993-1004)
+  // chi^T W_0 with W_0 = v_0 = ones / |ones| (sq.cpp:538-546, 993-1004); the
+  // mixed path may add a checkerboard, v_0 = (1 + c (-1)^(x+y+z)) / norm, whose
+  // overlap with the top of the stencil's spectrum lets lambda_max converge in
+  // fewer steps (|v|^2 = nw (1 + c^2) + 2c: one more even than odd point)
+  const double chk = a.lz_chk;
+  const double s0 = 1.0 / sqrt(nw * (1.0 + chk * chk) + 2.0 * chk);
   {
     PassIO<T> io;
     io.out = W[1];  // scratch: W[1] is overwritten before it is read
+    io.chk = chk;
     run_pass<T, C, PK_ONES>(a, S, dyn, io, mask, d0, d1);
-    const double s0 = 1.0 / sqrt(nw);
     for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) {
       S.pw_cur[p] = s0 * S.p_nxt[p];
       S.pw_prev[p] = 0.0;
@@ -1348,7 +1359,8 @@ __device__ void lanczos(const NodeArgs &a, NodeShared &S, unsigned char *dyn, co
     io.wout = W[m & 1];
     if (m == 0) {
       io.konst = 1;
-      io.sin = 1.0 / sqrt(nw);
+      io.chk = chk;
+      io.sin = s0;
     } else {
       io.vin = Y;
       io.p1 = W[(m - 1) & 1];

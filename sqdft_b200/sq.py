@@ -36,7 +36,7 @@ EXPORTS = [
     "sqb_lanczos_moments", "sqb_ne_constraint", "sqb_fermi_level", "sqb_density_energy",
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
-    "sqb_set_graph", "sqb_set_mixed_lanczos_tol",
+    "sqb_set_graph", "sqb_set_mixed_lanczos",
 ]
 
 
@@ -84,7 +84,7 @@ def library() -> C.CDLL:
         lib.sqb_create.argtypes = [C.POINTER(SqbGrid), C.c_int, C.POINTER(P)]
         lib.sqb_destroy.argtypes = [P]
         lib.sqb_set_precision.argtypes = [P, C.c_int]
-        lib.sqb_set_mixed_lanczos_tol.argtypes = [P, C.c_double]
+        lib.sqb_set_mixed_lanczos.argtypes = [P, C.c_double, C.c_double]
         lib.sqb_set_allreduce.argtypes = [P, ALLREDUCE_FN, C.c_void_p]
         lib.sqb_set_launch.argtypes = [P, C.c_int, C.c_int]
         lib.sqb_set_veff.argtypes = [P, _dp]
@@ -175,9 +175,10 @@ class Context:
     def set_precision(self, precision: int):
         _check(self.lib.sqb_set_precision(self.ptr, precision), "sqb_set_precision")
 
-    def set_mixed_lanczos_tol(self, tol: float):
-        """Lanczos stop and margin (Ha) of the FP32-mixed path (0: the grid's lanczos_tol)."""
-        _check(self.lib.sqb_set_mixed_lanczos_tol(self.ptr, float(tol)), "sqb_set_mixed_lanczos_tol")
+    def set_mixed_lanczos(self, tol: float = 0.0, checkerboard: float = 0.5):
+        """Lanczos of the FP32-mixed path: stop and margin in Ha (0: the grid's
+        lanczos_tol) and the checkerboard weight of the start vector."""
+        _check(self.lib.sqb_set_mixed_lanczos(self.ptr, float(tol), float(checkerboard)), "sqb_set_mixed_lanczos")
 
     def set_launch(self, ctas_per_sm: int = 0, cols_per_thread: int = 0):
         _check(self.lib.sqb_set_launch(self.ptr, ctas_per_sm, cols_per_thread), "sqb_set_launch")

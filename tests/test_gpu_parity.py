@@ -116,8 +116,9 @@ def test_mixed_precision_budget(golden, name):
 
 def test_mixed_loose_lanczos_budget():
     """The 110,592-node Al cell (31^3 windows, npl 96): with the Lanczos stop
-    at 1e-3 Ha the mixed path takes ~35 instead of 64 Lanczos steps per node
-    and its density stays within 1e-6 of max rho of the FP64 path's."""
+    at 1e-3 Ha and the checkerboard-weighted start the mixed path takes 24
+    instead of 64 Lanczos steps per node (35 from the constant start) and its
+    density stays within 1e-6 of max rho of the FP64 path's (4.9e-7)."""
     from sqdft_b200 import sq
     from sqdft_b200.cases import load
 
@@ -125,14 +126,14 @@ def test_mixed_loose_lanczos_budget():
     outs, iters = [], []
     for prec in (0, 1):
         with sq.Context(case, device=0, precision=prec) as ctx:
-            ctx.set_mixed_lanczos_tol(1e-3)
+            ctx.set_mixed_lanczos(1e-3)
             ctx.nonlocal_projectors()
             outs.append(ctx.spectral_quadrature(case.scf_iter, case.lambda_f))
             iters.append(ctx.stats()["lanczos_iters"])
     rel = np.abs(outs[1]["rho"] - outs[0]["rho"]).max() / np.abs(outs[0]["rho"]).max()
     print(f"mixed c2 (Lanczos stop 1e-3): rho {rel:.2e}, Lanczos steps {iters[1] / iters[0]:.2f} of FP64")
     assert rel <= 1e-6
-    assert iters[1] <= 0.65 * iters[0]
+    assert iters[1] <= 0.45 * iters[0]
     assert abs(outs[1]["Ebs"] - outs[0]["Ebs"]) / case.n_atm <= 1e-6
 
 
