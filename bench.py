@@ -7,17 +7,21 @@ Fermi-level solve, density and energies.  The default workload is the
 Chebyshev order 96) with the reference's own first-SCF-iteration Veff.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2]
-                    [--precision fp64|mixed] [--mixed-lanczos-tol T]
+                    [--precision both|fp64|mixed] [--mixed-lanczos-tol T]
                     [--impl ours|reference]
+
+The default (--precision both) times the FP32-mixed step (FP32 Lanczos vectors
+from a checkerboard-weighted start, Lanczos stop at T Ha, FP64 moments) and
+then the FP64 step, W untimed and K timed steps each; `value` is the mixed
+step, `fp64` the FP64 one, and `accuracy` the density, Fermi-level and band
+energy differences between the two arms' last steps.  --precision mixed
+alone states the error against one untimed FP64 step.
 
 value  nodes / (device time of the step), inputs resident in HBM
 e2e    nodes / (wall time of the C-ABI call with host buffers: Veff copied
        in from pinned memory, rho, rho_pj, Ci, chi, zee copied out)
 With N > 1 (torchrun, NCCL), rank r owns a z-slab of the grid; the
 Fermi-level sums and energies are all-reduced through the library's hook.
---precision mixed runs the FP32-mixed path (FP32 Lanczos vectors from a
-checkerboard-weighted start, stopping at T Ha; FP64 moments) and, outside the timed region, one FP64
-step of the same input to state the density error against it.
 --impl reference times the reference SQDFT compiled from its sources
 (oracle/_ref/sqref_driver: its LanczosAlgorithm and HsubTimesVec per node)
 on a node sample across all host threads.
@@ -130,11 +134,11 @@ def run_ours(args):
     torch.cuda.set_device(local)
     case = load_named(args.config)
     my = slab(case, rank, ws)
-    prec = sq.SQB_FP64 if args.precision == "fp64" else sq.SQB_FP32_MIXED
+    arms = {"both": ["mixed", "fp64"], "fp64": ["fp64"], "mixed": ["mixed"]}[args.precision]
+    first = sq.SQB_FP64 if arms[0] == "fp64" else sq.SQB_FP32_MIXED
 
-    ctx = sq.Context(my, device=local, precision=prec, allreduce=allreduce_fn(dist, "cuda") if ws > 1 else None)
-    if prec == sq.SQB_FP32_MIXED:
-        ctx.set_mixed_lanczos(args.mixed_lanczos_tol)
+    ctx = sq.Context(my, device=local, precision=first, allreduce=allreduce_fn(dist, "cuda") if ws > 1 else None)
+    ctx.set_mixed_lanczos(args.mixed_lanczos_tol)
     ctx.nonlocal_projectors()
     n = my.n_nodes
     K1 = my.npl + 1
@@ -147,8 +151,6 @@ def run_ours(args):
     import ctypes as C
 
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
-
-    st_ebs = [0.0]
 
     def step():
         flush.fill_(1)  # evict L2 (126 MB) between steps
@@ -166,80 +168,101 @@ def run_ours(args):
             raise sq.SQBError(rc, "sqb_spectral_quadrature")
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
-        st_ebs[0] = ebs.value
         st = ctx.stats()
         dev_ms = st["ms_lanczos_moments"] + st["ms_fermi"] + st["ms_density"]
-        return wall, dev_ms, st, lamv.value
+        return wall, dev_ms, st, lamv.value, ebs.value
 
-    for _ in range(args.warmup):
-        step()
-    walls, devs, node_ms = [], [], []
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            wall, dev_ms, st, lam = step()
-            walls.append(wall)
-            devs.append(dev_ms)
-            node_ms.append(st["ms_lanczos_moments"])
-    wall = float(np.mean(walls))
-    dev = float(np.mean(devs)) * 1e-3
-    kern = float(np.mean(node_ms)) * 1e-3
-    if ws > 1:
-        t = torch.tensor([wall, dev, kern], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        wall, dev, kern = t.tolist()
-    st = ctx.stats()
-    accuracy = None
-    if prec == sq.SQB_FP32_MIXED:  # untimed: the FP64 step on the same input
-        rho_mixed, lam_mixed, ebs_mixed = outs["rho"].copy(), lam, st_ebs[0]
-        ctx.set_precision(sq.SQB_FP64)
-        ref = ctx.spectral_quadrature(1, case.lambda_f)
-        ctx.set_precision(prec)
-        t = torch.tensor([np.abs(rho_mixed - ref["rho"].reshape(-1)).max(), np.abs(ref["rho"]).max()],
-                         dtype=torch.float64, device="cuda")
-        if ws > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        accuracy = {"rho_rel_err_vs_fp64": float(t[0] / t[1]), "lambda_f_diff": abs(lam_mixed - ref["lambda_f"]),
-                    "ebs_diff_per_atom": abs(ebs_mixed - ref["Ebs"]) / case.n_atm,
-                    "mixed_lanczos_tol": args.mixed_lanczos_tol}
-    traffic_per_node_step = None
+    peak, peak_kind = hbm_peak()
+    traffic = {}
     tr = ROOT / "profiles" / "node_kernel_traffic.json"
     if tr.exists():
-        traffic_per_node_step = json.loads(tr.read_text()).get(args.precision)
-    abytes = algorithmic_bytes(st, my, prec)
-    peak, peak_kind = hbm_peak()
-    achieved = abytes / kern / 1e9
-    steps_local = st["lanczos_iters"] + n + n * (my.npl // 2)
+        traffic = json.loads(tr.read_text())
+
+    def measure(arm):
+        """W untimed and K timed SQ steps of one precision; max over ranks."""
+        prec = sq.SQB_FP64 if arm == "fp64" else sq.SQB_FP32_MIXED
+        ctx.set_precision(prec)
+        for _ in range(args.warmup):
+            step()
+        walls, devs, node_ms = [], [], []
+        with ClockSampler(local) as clocks:
+            for _ in range(args.steps):
+                wall, dev_ms, st, lam, ebs = step()
+                walls.append(wall)
+                devs.append(dev_ms)
+                node_ms.append(st["ms_lanczos_moments"])
+        t = torch.tensor([np.mean(walls), np.mean(devs) * 1e-3, np.mean(node_ms) * 1e-3], dtype=torch.float64,
+                         device="cuda")
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall, dev, kern = t.tolist()
+        abytes = algorithmic_bytes(st, my, prec)
+        achieved = abytes / kern / 1e9
+        steps_local = st["lanczos_iters"] + n + n * (my.npl // 2)
+        per_step = traffic.get(arm)
+        return dict(prec=prec, wall=wall, dev=dev, kern=kern, st=st, lam=lam, ebs=ebs, rho=outs["rho"].copy(),
+                    clocks=clocks.summary(),
+                    roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                              "frac": achieved / peak, "peak_kind": peak_kind,
+                              "traffic": (per_step * steps_local) if per_step else None, "algorithmic_bytes": abytes,
+                              "kernel": "node_kernel", "kernel_ms": kern * 1e3})
+
+    res_arms = {arm: measure(arm) for arm in arms}
+    head = res_arms[arms[0]]
+    accuracy = None
+    if head["prec"] == sq.SQB_FP32_MIXED:
+        if "fp64" in res_arms:
+            ref = res_arms["fp64"]
+            ref_rho, ref_lam, ref_ebs = ref["rho"], ref["lam"], ref["ebs"]
+        else:  # untimed: the FP64 step on the same input
+            ctx.set_precision(sq.SQB_FP64)
+            r = ctx.spectral_quadrature(1, case.lambda_f)
+            ref_rho, ref_lam, ref_ebs = r["rho"].reshape(-1), r["lambda_f"], r["Ebs"]
+        t = torch.tensor([np.abs(head["rho"] - ref_rho).max(), np.abs(ref_rho).max()], dtype=torch.float64,
+                         device="cuda")
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        accuracy = {"rho_rel_err_vs_fp64": float(t[0] / t[1]), "lambda_f_diff": abs(head["lam"] - ref_lam),
+                    "ebs_diff_per_atom": abs(head["ebs"] - ref_ebs) / case.n_atm,
+                    "mixed_lanczos_tol": args.mixed_lanczos_tol, "lanczos_start": "1 + 0.5 (-1)^(x+y+z)"}
     res = None
     if rank == 0:
         nodes = case.n_nodes
         h2d = my.veff.nbytes * ws
         d2h = sum(a.nbytes for a in outs.values()) * ws
         cpu = cpu_baseline(args) if (ws == 1 and not args.no_cpu) else None
+        mixed = head["prec"] == sq.SQB_FP32_MIXED
+        st = head["st"]
         res = {
-            "metric": "SQ grid nodes/s (FP64 SQ step: Lanczos + Chebyshev moments + Fermi level + density)"
-            if prec == 0 else "SQ grid nodes/s (FP32-mixed SQ step: FP32 Lanczos vectors and a looser Lanczos "
-            "stop, FP64 moments + Fermi level + density)",
-            "value": nodes / dev, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64" if prec == 0 else "f32-mixed", "data": "synthetic (seeded-Gaussian-displaced FCC Al; "
-            "reference first-SCF Veff)",
+            "metric": "SQ grid nodes/s",
+            "step": "FP32-mixed SQ step at <= 1e-6 relative rho error vs FP64 (FP32 Lanczos vectors with a looser "
+            "Lanczos stop; FP64 Chebyshev moments, Fermi level, density)" if mixed else
+            "FP64 SQ step (Lanczos + Chebyshev moments + Fermi level + density)",
+            "value": nodes / head["dev"], "unit": "nodes/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["dev"] * 1e3, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32+f64 (mixed)" if mixed else "f64",
+            "data": "synthetic (seeded-Gaussian-displaced FCC Al; reference first-SCF Veff)",
             "config": {"workload": f"{args.config}: {case.n_int[0]}^3 grid, {nodes} nodes, {case.nw}^3 windows, "
                        f"npl {case.npl}, {case.n_atm} atoms", "nodes": nodes, "window": case.nw, "npl": case.npl,
-                       "precision": args.precision, "parallelism": f"z-slabs x{ws}", "l2": "flushed (256 MB write) "
+                       "precision": arms[0], "parallelism": f"z-slabs x{ws}", "l2": "flushed (256 MB write) "
                        "before every step"},
-            "e2e": {"value": nodes / wall, "unit": "nodes/s", "h2d_bytes_per_step": int(h2d),
+            "e2e": {"value": nodes / head["wall"], "unit": "nodes/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind,
-                         "traffic": (traffic_per_node_step * steps_local) if traffic_per_node_step else None,
-                         "algorithmic_bytes": abytes, "kernel": "node_kernel", "kernel_ms": kern * 1e3},
+            "roofline": head["roofline"],
             "gpu_launches": int(st["kernel_launches"]),
-            "clocks": clocks.summary(),
+            "clocks": head["clocks"],
             "lanczos_iters_per_node": st["lanczos_iters"] / n, "fermi_iters": st["fermi_iters"],
-            "lambda_f": lam,
+            "lambda_f": head["lam"],
         }
         if accuracy:
             res["accuracy"] = accuracy
+        if "fp64" in res_arms and arms[0] != "fp64":
+            f = res_arms["fp64"]
+            res["fp64"] = {"value": nodes / f["dev"], "e2e": nodes / f["wall"], "ms_per_step": f["dev"] * 1e3,
+                           "roofline": f["roofline"], "clocks": f["clocks"],
+                           "lanczos_iters_per_node": f["st"]["lanczos_iters"] / n,
+                           "gpu_launches": int(f["st"]["kernel_launches"])}
+            res["mixed_vs_fp64"] = f["dev"] / head["dev"]
         if cpu:
             res["cpu_baseline"] = cpu
     ctx.close()
@@ -300,8 +323,8 @@ def run_reference(args):
     desc = (f"{sample} nodes of {args.config} per step (reference LanczosAlgorithm + Chebyshev moment loop over "
             f"HsubTimesVec, g++ -O2), {threads} threads")
     print(json.dumps({
-        "impl": "reference", "metric": "SQ grid nodes/s (FP64 SQ step: Lanczos + Chebyshev moments + Fermi level + "
-        "density)", "value": v, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "impl": "reference", "metric": "SQ grid nodes/s",
+        "step": "reference FP64 per-node SQ work (LanczosAlgorithm + Chebyshev moment loop)", "value": v, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": sample / v * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded-Gaussian-displaced FCC Al; reference first-SCF Veff)",
         "config": {"workload": args.config, "precision": "fp64"},
@@ -315,7 +338,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c2")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--mixed-lanczos-tol", type=float, default=1e-3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=0)
