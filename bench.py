@@ -7,15 +7,20 @@ Fermi-level solve, density and energies.  The default workload is the
 Chebyshev order 96) with the reference's own first-SCF-iteration Veff.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2]
-                    [--precision both|fp64|mixed] [--mixed-lanczos-tol T]
+                    [--precision all|fp64|mixed|lq] [--mixed-lanczos-tol T]
                     [--impl ours|reference]
 
-The default (--precision both) times the FP32-mixed step (FP32 Lanczos vectors
-from a checkerboard-weighted start, Lanczos stop at T Ha, FP64 moments) and
-then the FP64 step, W untimed and K timed steps each; `value` is the mixed
-step, `fp64` the FP64 one, and `accuracy` the density, Fermi-level and band
-energy differences between the two arms' last steps.  --precision mixed
-alone states the error against one untimed FP64 step.
+The default (--precision all) times three forms of the step, W untimed and K
+timed steps each, and prints one line:
+  value       the FP64 Lanczos-quadrature step (SQB_FP64_LANCZOS_QUAD: bounds
+              and all Chebyshev moments of a node from one Lanczos run started
+              at the node, Lanczos stop at T Ha)
+  fp32_mixed  the FP32-mixed step (FP32 Lanczos vectors from a checkerboard-
+              weighted start, stop at T Ha; FP64 Chebyshev moments)
+  fp64        the FP64 parity step
+`accuracy` holds each fast form's density, Fermi-level and band-energy
+differences from the FP64 arm's last step.  --precision lq|mixed alone states
+them against one untimed FP64 step.
 
 value  nodes / (device time of the step), inputs resident in HBM
 e2e    nodes / (wall time of the C-ABI call with host buffers: Veff copied
@@ -105,7 +110,7 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def algorithmic_bytes(stats, case, precision):
+def algorithmic_bytes(stats, case, precision, lq=False):
     """Bytes per node-kernel launch by the roofline's accounting: per matvec
     step n_w (3 s_v + s_V) plus the projector tables of every atom whose ball
     meets the window, steps = Lanczos iterations + 1 + npl/2 per node.  Veff
@@ -114,7 +119,7 @@ def algorithmic_bytes(stats, case, precision):
     nw = stats["window_points"]
     n = case.n_nodes
     lz_steps = stats["lanczos_iters"] + n
-    ch_steps = n * (case.npl // 2)
+    ch_steps = 0 if lq else n * (case.npl // 2)
     sv_lz = 8 if precision == 0 else 4
     proj_lz = stats["proj_points"] - stats["proj_points_cheb"]
     return (lz_steps * nw * (3 * sv_lz + 8) + proj_lz * 8) + (ch_steps * nw * 32 + stats["proj_points_cheb"] * 8)
@@ -134,8 +139,9 @@ def run_ours(args):
     torch.cuda.set_device(local)
     case = load_named(args.config)
     my = slab(case, rank, ws)
-    arms = {"both": ["mixed", "fp64"], "fp64": ["fp64"], "mixed": ["mixed"]}[args.precision]
-    first = sq.SQB_FP64 if arms[0] == "fp64" else sq.SQB_FP32_MIXED
+    arms = {"all": ["lq", "mixed", "fp64"], "fp64": ["fp64"], "mixed": ["mixed"], "lq": ["lq"]}[args.precision]
+    prec_of = {"fp64": sq.SQB_FP64, "mixed": sq.SQB_FP32_MIXED, "lq": sq.SQB_FP64_LANCZOS_QUAD}
+    first = prec_of[arms[0]]
 
     ctx = sq.Context(my, device=local, precision=first, allreduce=allreduce_fn(dist, "cuda") if ws > 1 else None)
     ctx.set_mixed_lanczos(args.mixed_lanczos_tol)
@@ -180,7 +186,7 @@ def run_ours(args):
 
     def measure(arm):
         """W untimed and K timed SQ steps of one precision; max over ranks."""
-        prec = sq.SQB_FP64 if arm == "fp64" else sq.SQB_FP32_MIXED
+        prec = prec_of[arm]
         ctx.set_precision(prec)
         for _ in range(args.warmup):
             step()
@@ -196,9 +202,9 @@ def run_ours(args):
         if ws > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         wall, dev, kern = t.tolist()
-        abytes = algorithmic_bytes(st, my, prec)
+        abytes = algorithmic_bytes(st, my, prec, lq=(arm == "lq"))
         achieved = abytes / kern / 1e9
-        steps_local = st["lanczos_iters"] + n + n * (my.npl // 2)
+        steps_local = st["lanczos_iters"] + n + (0 if arm == "lq" else n * (my.npl // 2))
         per_step = traffic.get(arm)
         return dict(prec=prec, wall=wall, dev=dev, kern=kern, st=st, lam=lam, ebs=ebs, rho=outs["rho"].copy(),
                     clocks=clocks.summary(),
@@ -209,38 +215,46 @@ def run_ours(args):
 
     res_arms = {arm: measure(arm) for arm in arms}
     head = res_arms[arms[0]]
-    accuracy = None
-    if head["prec"] == sq.SQB_FP32_MIXED:
+
+    def accuracy_of(arm):
+        """Differences of an arm's last step from the FP64 arm's (or from one
+        untimed FP64 step when the FP64 arm is not run)."""
+        r = res_arms[arm]
         if "fp64" in res_arms:
             ref = res_arms["fp64"]
             ref_rho, ref_lam, ref_ebs = ref["rho"], ref["lam"], ref["ebs"]
-        else:  # untimed: the FP64 step on the same input
+        else:
             ctx.set_precision(sq.SQB_FP64)
-            r = ctx.spectral_quadrature(1, case.lambda_f)
-            ref_rho, ref_lam, ref_ebs = r["rho"].reshape(-1), r["lambda_f"], r["Ebs"]
-        t = torch.tensor([np.abs(head["rho"] - ref_rho).max(), np.abs(ref_rho).max()], dtype=torch.float64,
+            out = ctx.spectral_quadrature(1, case.lambda_f)
+            ref_rho, ref_lam, ref_ebs = out["rho"].reshape(-1), out["lambda_f"], out["Ebs"]
+        t = torch.tensor([np.abs(r["rho"] - ref_rho).max(), np.abs(ref_rho).max()], dtype=torch.float64,
                          device="cuda")
         if ws > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        accuracy = {"rho_rel_err_vs_fp64": float(t[0] / t[1]), "lambda_f_diff": abs(head["lam"] - ref_lam),
-                    "ebs_diff_per_atom": abs(head["ebs"] - ref_ebs) / case.n_atm,
-                    "mixed_lanczos_tol": args.mixed_lanczos_tol, "lanczos_start": "1 + 0.5 (-1)^(x+y+z)"}
+        return {"rho_rel_err_vs_fp64": float(t[0] / t[1]), "lambda_f_diff": abs(r["lam"] - ref_lam),
+                "ebs_diff_per_atom": abs(r["ebs"] - ref_ebs) / case.n_atm, "lanczos_tol": args.mixed_lanczos_tol}
+
+    acc = {arm: accuracy_of(arm) for arm in arms if arm != "fp64"}
+    steps_desc = {
+        "fp64": "FP64 SQ step (Lanczos bounds + Chebyshev moments + Fermi level + density), the parity path",
+        "mixed": "FP32-mixed SQ step (FP32 Lanczos vectors from a checkerboard-weighted start, looser Lanczos stop; "
+                 "FP64 Chebyshev moments, Fermi level, density)",
+        "lq": "FP64 Lanczos-quadrature SQ step (bounds and all Chebyshev moments from one Lanczos run per node "
+              "through the Gauss-quadrature identity, looser Lanczos stop; Fermi level, density)",
+    }
     res = None
     if rank == 0:
         nodes = case.n_nodes
         h2d = my.veff.nbytes * ws
         d2h = sum(a.nbytes for a in outs.values()) * ws
         cpu = cpu_baseline(args) if (ws == 1 and not args.no_cpu) else None
-        mixed = head["prec"] == sq.SQB_FP32_MIXED
         st = head["st"]
         res = {
             "metric": "SQ grid nodes/s",
-            "step": "FP32-mixed SQ step at <= 1e-6 relative rho error vs FP64 (FP32 Lanczos vectors with a looser "
-            "Lanczos stop; FP64 Chebyshev moments, Fermi level, density)" if mixed else
-            "FP64 SQ step (Lanczos + Chebyshev moments + Fermi level + density)",
+            "step": steps_desc[arms[0]] + (" at <= 1e-6 relative rho error vs FP64" if arms[0] != "fp64" else ""),
             "value": nodes / head["dev"], "unit": "nodes/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["dev"] * 1e3, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "f32+f64 (mixed)" if mixed else "f64",
+            "vs_baseline": None, "dtype": "f32+f64 (mixed)" if arms[0] == "mixed" else "f64",
             "data": "synthetic (seeded-Gaussian-displaced FCC Al; reference first-SCF Veff)",
             "config": {"workload": f"{args.config}: {case.n_int[0]}^3 grid, {nodes} nodes, {case.nw}^3 windows, "
                        f"npl {case.npl}, {case.n_atm} atoms", "nodes": nodes, "window": case.nw, "npl": case.npl,
@@ -254,15 +268,19 @@ def run_ours(args):
             "lanczos_iters_per_node": st["lanczos_iters"] / n, "fermi_iters": st["fermi_iters"],
             "lambda_f": head["lam"],
         }
-        if accuracy:
-            res["accuracy"] = accuracy
+        if arms[0] in acc:
+            res["accuracy"] = acc[arms[0]]
+        for arm in arms[1:]:
+            f = res_arms[arm]
+            sub = {"step": steps_desc[arm], "value": nodes / f["dev"], "e2e": nodes / f["wall"],
+                   "ms_per_step": f["dev"] * 1e3, "roofline": f["roofline"], "clocks": f["clocks"],
+                   "lanczos_iters_per_node": f["st"]["lanczos_iters"] / n,
+                   "gpu_launches": int(f["st"]["kernel_launches"])}
+            if arm in acc:
+                sub["accuracy"] = acc[arm]
+            res[{"fp64": "fp64", "mixed": "fp32_mixed", "lq": "lanczos_quadrature"}[arm]] = sub
         if "fp64" in res_arms and arms[0] != "fp64":
-            f = res_arms["fp64"]
-            res["fp64"] = {"value": nodes / f["dev"], "e2e": nodes / f["wall"], "ms_per_step": f["dev"] * 1e3,
-                           "roofline": f["roofline"], "clocks": f["clocks"],
-                           "lanczos_iters_per_node": f["st"]["lanczos_iters"] / n,
-                           "gpu_launches": int(f["st"]["kernel_launches"])}
-            res["mixed_vs_fp64"] = f["dev"] / head["dev"]
+            res["speedup_vs_fp64"] = res_arms["fp64"]["dev"] / head["dev"]
         if cpu:
             res["cpu_baseline"] = cpu
     ctx.close()
@@ -338,7 +356,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c2")
-    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
+    ap.add_argument("--precision", default="all", choices=["all", "fp64", "mixed", "lq"])
     ap.add_argument("--mixed-lanczos-tol", type=float, default=1e-3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=0)

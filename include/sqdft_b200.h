@@ -48,6 +48,14 @@ extern "C" {
                              the Chebyshev moments, coefficients, Fermi solve and
                              assembly in FP64.  Lanczos stops at
                              max(lanczos_tol, sqb_set_mixed_lanczos tol). */
+#define SQB_FP64_LANCZOS_QUAD 2 /* FP64; bounds and Chebyshev moments of each node
+                             from one Lanczos run started at the node's unit
+                             vector: its tridiagonal T_m gives mu_j = e_1^T
+                             T_j((T_m - chi)/zee) e_1 exactly for j <= 2m - 1
+                             (m >= npl/2 + 1 steps), its extreme Ritz values
+                             the bounds (stop and margin as for SQB_FP32_MIXED).
+                             Same moments as the reference at slightly
+                             different bounds; no counterpart in the reference. */
 
 typedef struct sqb_ctx sqb_ctx;
 

@@ -159,7 +159,8 @@ void fill_node_args(sqb_ctx *c, NodeArgs &a) {
   a.npl = c->g.npl;
   a.h3 = c->h3;
   a.mixed = c->precision == SQB_FP32_MIXED;
-  a.lanczos_tol = a.mixed ? std::max(c->g.lanczos_tol, c->mixed_lanczos_tol) : c->g.lanczos_tol;
+  a.lq = c->precision == SQB_FP64_LANCZOS_QUAD;
+  a.lanczos_tol = (a.mixed || a.lq) ? std::max(c->g.lanczos_tol, c->mixed_lanczos_tol) : c->g.lanczos_tol;
   a.lz_chk = a.mixed ? c->mixed_lanczos_chk : 0.0;
   for (int k = 0; k <= FDN; k++) {
     a.coeff_lap[k] = c->g.coeff_lap[k];
@@ -477,7 +478,8 @@ int sqb_destroy(sqb_ctx *c) {
 }
 
 int sqb_set_precision(sqb_ctx *c, int precision) {
-  if (!c || (precision != SQB_FP64 && precision != SQB_FP32_MIXED)) return SQB_ERR_ARG;
+  if (!c || (precision != SQB_FP64 && precision != SQB_FP32_MIXED && precision != SQB_FP64_LANCZOS_QUAD))
+    return SQB_ERR_ARG;
   c->precision = precision;
   drop_graph(c);
   return SQB_OK;
@@ -784,7 +786,7 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   c->stats.lanczos_iters = sum;
   c->stats.max_lanczos_iters = mx;
   // passes: Lanczos 2 per iteration + 2, Chebyshev npl/2 (matvec passes only)
-  c->stats.matvecs = sum + (long long)N + (long long)N * (c->g.npl / 2);
+  c->stats.matvecs = sum + (long long)N + (c->precision == SQB_FP64_LANCZOS_QUAD ? 0LL : (long long)N * (c->g.npl / 2));
   c->stats.proj_points = (long long)pp[0];
   c->stats.proj_points_cheb = (long long)pp[1];
   if (lanczos_iters) std::memcpy(lanczos_iters, its.data(), N * sizeof(int));

@@ -49,7 +49,8 @@ constexpr int VJP_K = 8;  // adjoint: checkpoint every VJP_K recursion vectors
 
 struct NodeArgs {
   int mode;
-  int mixed;     // 1: Chebyshev passes in FP32
+  int mixed;     // 1: FP32-mixed path (FP32 Lanczos vectors, FP32 force recursion)
+  int lq;        // 1: bounds and moments from one Lanczos run at the node (Gauss-quadrature identity)
   int n;         // window edge 2*nloc+1
   int nloc;
   int np[3];
@@ -105,8 +106,10 @@ cudaError_t setup_node_forces(int n);
 cudaError_t launch_node_forces(const NodeArgs &a, int grid, int cols, cudaStream_t s);
 cudaError_t setup_node_vjp(int n);
 cudaError_t setup_node_sq32(int n);
+cudaError_t setup_node_lq(int n);
 cudaError_t launch_node_vjp(const NodeArgs &a, int grid, int cols, cudaStream_t s);
 cudaError_t launch_node_sq32(const NodeArgs &a, int grid, int cols, cudaStream_t s);
+cudaError_t launch_node_lq(const NodeArgs &a, int grid, int cols, cudaStream_t s);
 cudaError_t node_kernel_setup(int n);
 // Stage size wanted for a per-plane footprint of `elems` values (the launcher
 // clamps it to what the launch's shared memory leaves).

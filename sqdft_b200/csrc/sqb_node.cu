@@ -69,6 +69,7 @@ cudaError_t node_kernel_setup(int n) {
   if (e == cudaSuccess) e = setup_node_forces(n);
   if (e == cudaSuccess) e = setup_node_vjp(n);
   if (e == cudaSuccess) e = setup_node_sq32(n);
+  if (e == cudaSuccess) e = setup_node_lq(n);
   return e;
 }
 
@@ -76,6 +77,7 @@ cudaError_t launch_node_kernel(const NodeArgs &args, int grid, int cols, cudaStr
   if (args.mode == MODE_FORCES) return launch_node_forces(args, grid, cols, s);
   if (args.mode == MODE_VJP) return launch_node_vjp(args, grid, cols == -2 ? 0 : cols, s);
   if (args.mixed && args.mode == MODE_SQ) return launch_node_sq32(args, grid, cols, s);
+  if (args.lq && args.mode == MODE_SQ) return launch_node_lq(args, grid, cols, s);
   return launch_kind<KIND_SQ>(args, grid, cols, s);
 }
 

@@ -42,7 +42,7 @@ namespace sqb {
 // node_kernel_setup.
 extern int g_smem_optin;
 
-enum : int { KIND_SQ = 0, KIND_FORCES = 1, KIND_VJP = 2, KIND_SQ32 = 3 };
+enum : int { KIND_SQ = 0, KIND_FORCES = 1, KIND_VJP = 2, KIND_SQ32 = 3, KIND_LQ = 4 };
 
 namespace {
 
@@ -1416,6 +1416,147 @@ __device__ void lanczos(const NodeArgs &a, NodeShared &S, unsigned char *dyn, co
   count_proj_points(a, S, S.count + 1, 0);  // Lanczos: iterations + the first matvec
 }
 
+// Moments and bounds from one FP64 Lanczos run started at the node's unit
+// vector e_c (the quantities of sq.cpp:564-655, computed another way).  With
+// Q_m the Lanczos basis (q_1 = e_c) and T_m its tridiagonal, p(H) e_c = Q_m
+// p(T_m) e_1 for degree < m, hence e_c^T p(H) e_c = e_1^T p(T_m) e_1 for
+// degree <= 2m - 1 (the Gauss-quadrature identity): m >= npl/2 + 1 steps give
+// every Chebyshev moment mu_j = e_c^T T_j((H - chi)/zee) e_c, j <= npl, at any
+// bounds, from a recurrence on the m x m tridiagonal.  The bounds are the
+// extreme Ritz values of T_m -/+ lanczos_tol once both move by less than
+// lanczos_tol between steps (sq.cpp:1050-1092's test), which for high npl the
+// npl/2 + 1 steps usually already meet.  One sweep per step replaces the
+// Lanczos sweeps for the bounds plus the npl/2 Chebyshev sweeps.
+template <int C>
+__device__ void lanczos_quadrature(const NodeArgs &a, NodeShared &S, unsigned char *dyn,
+                                   const uint32_t (&mask)[4], double &lmin_out, double &lmax_out, int &iters,
+                                   double *mu) {
+  const int n = a.n;
+  const int kmin = a.npl / 2 + 1;
+  double *Y = slot<double>(a, 0);
+  double *W[2] = {slot<double>(a, 1), slot<double>(a, 2)};
+  double d0 = 0.0, d1 = 0.0;
+  {  // e_c into Y, and chi^T e_c
+    PassIO<double> io;
+    io.out = Y;
+    run_pass<double, C, PK_DELTA>(a, S, dyn, io, mask, d0, d1);
+    for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) {
+      S.pw_cur[p] = S.p_nxt[p];
+      S.pw_prev[p] = 0.0;
+      S.p_cur[p] = S.pw_cur[p] / S.p_den[p];
+      S.p_nxt[p] = 0.0;
+    }
+    __syncthreads();
+  }
+  double a_prev = 0.0, s_prev = 1.0, bs_prev = 0.0;
+  double lmin_prev = 0.0, lmax_prev = 0.0;
+  if (threadIdx.x == 0) {
+    S.count = 0;
+    S.stop = 0;
+  }
+  __syncthreads();
+  for (int m = 0;; m++) {
+    PassIO<double> io;
+    io.out = Y;
+    io.wout = W[m & 1];
+    io.vin = Y;
+    if (m == 0) {  // W_0 = 1 (e_c - 0 e_c) - 0 e_c, exactly e_c
+      io.p1 = Y;
+      io.p2 = Y;
+      io.s1 = 1.0;
+    } else {
+      io.p1 = W[(m - 1) & 1];
+      io.p2 = m >= 2 ? W[m & 1] : W[(m - 1) & 1];
+      io.s1 = s_prev;
+      io.ca = a_prev;
+      io.cb = bs_prev;
+    }
+    d0 = 0.0;
+    d1 = 0.0;
+    run_pass<double, C, PK_LZF>(a, S, dyn, io, mask, d0, d1);
+    block_sum3(S, d0, d1, 0.0);
+    const double bm = m == 0 ? 1.0 : sqrt(S.scal[0]);
+    const double am = S.scal[1] / (bm * bm);
+    const double sm = 1.0 / bm;
+    if (threadIdx.x == 0) {
+      S.aa[m] = am;
+      if (m > 0) S.bb[m - 1] = bm;
+    }
+    const double bs_cur = m == 0 ? 0.0 : bm * s_prev;
+    for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) {
+      const double nx = sm * (S.p_nxt[p] - am * S.pw_cur[p]) - bs_cur * S.pw_prev[p];
+      S.pw_prev[p] = S.pw_cur[p];
+      S.pw_cur[p] = nx;
+      S.p_cur[p] = nx / S.p_den[p];
+      S.p_nxt[p] = 0.0;
+    }
+    __syncthreads();
+    a_prev = am;
+    bs_prev = bs_cur;
+    s_prev = sm;
+    // after sweep m the tridiagonal T_m+1 is complete; the convergence test
+    // starts once it has the npl/2 + 1 rows the moments need
+    if (m + 1 < kmin) continue;
+    tridiag_extremes(S, m + 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const double lmin = S.eig[0], lmax = S.eig[1];
+      const bool first = (m + 1 == kmin);
+      const double dl = fabs(lmin - lmin_prev), dm = fabs(lmax - lmax_prev);
+      lmin_prev = lmin;
+      lmax_prev = lmax;
+      S.count = m + 1;  // rows of T
+      S.stop = !first && !(S.count < LANCZOS_MAX_ITER && (dl > a.lanczos_tol || dm > a.lanczos_tol));
+      if (S.count >= LANCZOS_MAX_ITER) {
+        S.stop = 1;
+        atomicOr(a.status, ST_LANCZOS_MAXITER);
+      }
+    }
+    __syncthreads();
+    if (S.stop) break;
+  }
+  const int k = S.count;
+  lmin_out = S.eig[0] - a.lanczos_tol;
+  lmax_out = S.eig[1] + a.lanczos_tol;
+  iters = k - 1;  // matvecs = iters + 1, as for the reference's Lanczos
+  count_proj_points(a, S, k, 0);
+  // mu_j = e_1^T T_j(That) e_1, That = (T_k - chi) / zee: the Chebyshev
+  // recurrence on k-vectors, one warp, in the (now free) window-vector slots
+  // (k <= n^3: Lanczos on the window cannot take more steps than its size)
+  const double chi = 0.5 * (lmax_out + lmin_out), zee = 0.5 * (lmax_out - lmin_out);
+  if (threadIdx.x < 32 && (long long)k <= (long long)n * n * n) {
+    const int lane = threadIdx.x;
+    double *v0 = Y, *v1 = W[0], *v2 = W[1];
+    for (int i = lane; i < k; i += 32) {
+      v0[i] = i == 0 ? 1.0 : 0.0;
+      v1[i] = i == 0 ? (S.aa[0] - chi) / zee : (i == 1 ? S.bb[0] / zee : 0.0);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      mu[0] = 1.0 / a.h3;
+      mu[1] = v1[0] / a.h3;
+    }
+    for (int j = 1; j < a.npl; j++) {
+      for (int i = lane; i < k; i += 32) {
+        double t = (S.aa[i] - chi) / zee * v1[i];
+        if (i > 0) t += S.bb[i - 1] / zee * v1[i - 1];
+        if (i + 1 < k) t += S.bb[i] / zee * v1[i + 1];
+        v2[i] = 2.0 * t - v0[i];
+      }
+      __syncwarp();
+      if (lane == 0) mu[j + 1] = v2[0] / a.h3;
+      double *tt = v0;
+      v0 = v1;
+      v1 = v2;
+      v2 = tt;
+      __syncwarp();
+    }
+  } else if (threadIdx.x == 0 && (long long)k > (long long)n * n * n) {
+    atomicOr(a.status, ST_LANCZOS_MAXITER);
+  }
+  __syncthreads();
+}
+
 // Chebyshev moments (sq.cpp:564-655) in precision T.
 template <typename T, int C>
 __device__ void moments(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const uint32_t (&mask)[4],
@@ -1853,7 +1994,19 @@ __global__ void __launch_bounds__(MAXT, 1) node_kernel(NodeArgs a) {
       build_items(a, S, row_items(a, dyn));
       __syncthreads();
     }
-    if constexpr (KIND == KIND_SQ || KIND == KIND_SQ32) {
+    if constexpr (KIND == KIND_LQ) {
+      double lmin = 0.0, lmax = 0.0;
+      int iters = 0;
+      double *mu = a.rho_pj + (size_t)node * (a.npl + 1);
+      lanczos_quadrature<C>(a, S, dyn, mask, lmin, lmax, iters, mu);
+      if (threadIdx.x == 0) {
+        a.chi[node] = 0.5 * (lmax + lmin);
+        a.zee[node] = 0.5 * (lmax - lmin);
+        if (a.lmin) a.lmin[node] = lmin;
+        if (a.lmax) a.lmax[node] = lmax;
+        if (a.lanczos_iters) a.lanczos_iters[node] = iters;
+      }
+    } else if constexpr (KIND == KIND_SQ || KIND == KIND_SQ32) {
       using TV = typename std::conditional<KIND == KIND_SQ32, float, double>::type;
       if (a.mode == MODE_SQ || a.mode == MODE_MOMENTS) {
         // SQ: Lanczos bounds then moments; MODE_MOMENTS: moments with given bounds

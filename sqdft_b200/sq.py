@@ -24,6 +24,7 @@ LIB_PATH = Path(os.environ.get("SQDFT_B200_LIB", HERE / "_build" / "libsqdft_b20
 
 SQB_FP64 = 0
 SQB_FP32_MIXED = 1
+SQB_FP64_LANCZOS_QUAD = 2
 SQB_SUM, SQB_MIN, SQB_MAX = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)

@@ -201,3 +201,62 @@ def test_graph_replay_matches_plain_launches(golden):
         assert np.array_equal(r["rho_pj"], plain["rho_pj"])
     assert np.array_equal(moved["rho_pj"], moved_plain["rho_pj"])
     assert not np.array_equal(moved["rho_pj"], plain["rho_pj"])
+
+
+@pytest.mark.parametrize("name", ["tiny", "lihs", "mid"])
+def test_lanczos_quadrature_moments_identity(golden, name):
+    """SQB_FP64_LANCZOS_QUAD: the moments its one Lanczos run gives through the
+    Gauss-quadrature identity equal the Chebyshev recursion's (sq.cpp:564-655)
+    at the same bounds, to rounding."""
+    from sqdft_b200 import sq
+
+    case, _ = golden(name)
+    with _ctx(case, precision=sq.SQB_FP64_LANCZOS_QUAD) as ctx:
+        m = ctx.lanczos_moments()
+        ctx.set_precision(sq.SQB_FP64)
+        cheb = ctx.moments_at(m["chi"], m["zee"])
+    rel = np.abs(m["rho_pj"] - cheb).max() / np.abs(cheb).max()
+    print(f"Lanczos-quadrature moments vs Chebyshev at the same bounds ({name}): {rel:.2e}")
+    assert rel <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["tiny", "mid"])
+def test_lanczos_quadrature_budget(golden, name):
+    """At the grid's Lanczos tolerance its bounds (the Ritz values of the run
+    from e_c) differ from the reference's by ~1e-5 Ha, which moves rho by
+    ~3e-7 of max rho here."""
+    from sqdft_b200 import sq
+
+    case, ref = golden(name)
+    with _ctx(case, precision=sq.SQB_FP64_LANCZOS_QUAD) as ctx:
+        out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+        f = ctx.forces_nonlocal()
+    rel = np.abs(out["rho"] - ref["rho"]).max() / np.abs(ref["rho"]).max()
+    ebs = abs(out["Ebs"] - ref["Ebs"][0]) / case.n_atm
+    print(f"Lanczos quadrature {name}: rho {rel:.2e} Ebs {ebs:.1e} Ha/atom F {np.abs(f - ref['fnloc']).max():.1e}")
+    assert rel <= 1e-6
+    assert ebs <= 1e-6
+    assert np.abs(f - ref["fnloc"]).max() <= 1e-6
+
+
+def test_lanczos_quadrature_c2():
+    """The 110,592-node Al cell (npl 96) with the Lanczos stop at 1e-3 Ha: 50
+    Lanczos steps per node give bounds and all 97 moments (the FP64 path takes
+    65 Lanczos plus 49 Chebyshev sweeps); rho within 1e-6 of max rho of the
+    FP64 path's (2.5e-7 measured)."""
+    from sqdft_b200 import sq
+    from sqdft_b200.cases import load
+
+    case = load("c2")
+    outs, st = [], []
+    for prec in (sq.SQB_FP64, sq.SQB_FP64_LANCZOS_QUAD):
+        with sq.Context(case, device=0, precision=prec) as ctx:
+            ctx.set_mixed_lanczos(1e-3)
+            ctx.nonlocal_projectors()
+            outs.append(ctx.spectral_quadrature(case.scf_iter, case.lambda_f))
+            st.append(ctx.stats())
+    rel = np.abs(outs[1]["rho"] - outs[0]["rho"]).max() / np.abs(outs[0]["rho"]).max()
+    print(f"Lanczos quadrature c2 (stop 1e-3): rho {rel:.2e}, matvecs {st[1]['matvecs'] / st[0]['matvecs']:.2f} of FP64")
+    assert rel <= 1e-6
+    assert st[1]["matvecs"] <= 0.5 * st[0]["matvecs"]
+    assert abs(outs[1]["lambda_f"] - outs[0]["lambda_f"]) <= 1e-6
