@@ -122,15 +122,16 @@ typedef struct sqb_stats {
 int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out);
 int sqb_destroy(sqb_ctx *ctx);
 int sqb_set_precision(sqb_ctx *ctx, int precision);
-/* Lanczos of the FP32-mixed path.  tol: stopping tolerance (Ha), also the
- * margin put around its Ritz values (sq.cpp:1050-1092 with this tolerance);
- * default 0, i.e. sqb_grid.lanczos_tol.  The density's sensitivity to the
- * bounds falls with npl: a looser stop suits high-order expansions only.
- * checkerboard in [0, 1]: start vector 1 + c (-1)^(x+y+z), normalised, in
- * place of the reference's constant vector (sq.cpp:538-546); its overlap
- * with the top of the spectrum speeds the convergence of lambda_max;
- * default 0.5.  The FP64 path always uses the reference's start vector and
- * sqb_grid.lanczos_tol.  No counterpart in the reference. */
+/* Lanczos of the FP32-mixed and Lanczos-quadrature forms.  tol: stopping
+ * tolerance (Ha), also the margin put around the Ritz values (sq.cpp:1050-1092
+ * with this tolerance); default 0, i.e. sqb_grid.lanczos_tol.  The density's
+ * sensitivity to the bounds falls with npl: a looser stop suits high-order
+ * expansions only.  checkerboard in [0, 1] (FP32-mixed form): start vector
+ * 1 + c (-1)^(x+y+z), normalised, in place of the reference's constant vector
+ * (sq.cpp:538-546); its overlap with the top of the spectrum speeds the
+ * convergence of lambda_max; default 0.5.  The FP64 path always uses the
+ * reference's start vector and sqb_grid.lanczos_tol.  No counterpart in the
+ * reference. */
 int sqb_set_mixed_lanczos(sqb_ctx *ctx, double tol, double checkerboard);
 int sqb_set_allreduce(sqb_ctx *ctx, sqb_allreduce_fn fn, void *user);
 /* Launch shape of the node kernel: persistent CTAs per SM, and the layout of

@@ -12,7 +12,10 @@
 // Failures print the reference's message and exit(1), as the reference does.
 //
 // Environment:
-//   SQDFT_B200_PRECISION=fp32   FP32-mixed recursion (default FP64)
+//   SQDFT_B200_PRECISION=fp32   FP32-mixed form (default FP64, the parity path)
+//   SQDFT_B200_PRECISION=lq     FP64 Lanczos-quadrature form
+//   SQDFT_B200_LANCZOS_TOL=T    Lanczos stop (Ha) of the two forms above
+//                               (default: the input's lanczos_tol)
 //   SQDFT_B200_DEVICE=k         CUDA device (default: MPI rank)
 //   SQDFT_B200_EXPORT=path      at the first SQ call, write the SQ inputs as a
 //                               case container (sqdft_b200/csrc/sq_case.h) and
@@ -83,6 +86,11 @@ void ensure_ctx(DS_SQ *p) {
   if (rc) fail(rc, "sqb_create");
   const char *prec = std::getenv("SQDFT_B200_PRECISION");
   if (prec && (!std::strcmp(prec, "fp32") || !std::strcmp(prec, "mixed"))) sqb_set_precision(g_ctx, SQB_FP32_MIXED);
+  if (prec && !std::strcmp(prec, "lq")) sqb_set_precision(g_ctx, SQB_FP64_LANCZOS_QUAD);
+  if (const char *tol = std::getenv("SQDFT_B200_LANCZOS_TOL")) {
+    rc = sqb_set_mixed_lanczos(g_ctx, std::atof(tol), 0.5);
+    if (rc) fail(rc, "sqb_set_mixed_lanczos");
+  }
   if (p->nproc > 1) sqb_set_allreduce(g_ctx, mpi_reduce, nullptr);
   std::atexit(destroy_ctx);
 }
