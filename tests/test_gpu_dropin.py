@@ -73,3 +73,20 @@ def test_dropin_program_reproduces_reference_run(tmp_path):
     assert got["fermi_iters"] == g["fermi_iters"]
     assert abs(got["free_energy"] - g["free_energy"]) <= 1e-8
     assert np.abs(np.array(got["forces"]) - np.array(g["forces"])).max() <= 1e-7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp32", "lq"])
+def test_dropin_program_fast_forms(tmp_path, precision):
+    """The whole program with the FP32-mixed or the Lanczos-quadrature SQ step
+    (at the input's Lanczos tolerance) converges like the reference run: the
+    same number of SCF iterations, the free energy within 1e-6 Ha/atom and the
+    forces within 1e-5 Ha/bohr."""
+    g = json.loads(GOLDEN.read_text())
+    got = run_program(tmp_path, precision)
+    de = abs(got["free_energy"] - g["free_energy"])
+    df = np.abs(np.array(got["forces"]) - np.array(g["forces"])).max()
+    print(f"drop-in {precision}: {len(got['scf'])} SCF iterations, free energy {de:.1e} Ha/atom, forces {df:.1e}")
+    assert len(got["scf"]) == len(g["scf"])
+    assert de <= 1e-6
+    assert df <= 1e-5
