@@ -1494,14 +1494,15 @@ __device__ void lanczos_quadrature(const NodeArgs &a, NodeShared &S, unsigned ch
     a_prev = am;
     bs_prev = bs_cur;
     s_prev = sm;
-    // after sweep m the tridiagonal T_m+1 is complete; the convergence test
-    // starts once it has the npl/2 + 1 rows the moments need
-    if (m + 1 < kmin) continue;
+    // after sweep m the tridiagonal T_m+1 is complete; its extremes are
+    // followed from npl/2 rows on, so that the run can stop at the npl/2 + 1
+    // rows the moments need when the bounds have settled by then
+    if (m + 2 < kmin) continue;
     tridiag_extremes(S, m + 1);
     __syncthreads();
     if (threadIdx.x == 0) {
       const double lmin = S.eig[0], lmax = S.eig[1];
-      const bool first = (m + 1 == kmin);
+      const bool first = (m + 2 == kmin);
       const double dl = fabs(lmin - lmin_prev), dm = fabs(lmax - lmax_prev);
       lmin_prev = lmin;
       lmax_prev = lmax;
