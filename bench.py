@@ -175,7 +175,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         st = ctx.stats()
-        dev_ms = st["ms_lanczos_moments"] + st["ms_fermi"] + st["ms_density"]
+        dev_ms = st["ms_lanczos_moments"] + st["ms_fermi"] + st["ms_density"] + st["ms_defect"]
         return wall, dev_ms, st, lamv.value, ebs.value
 
     peak, peak_kind = hbm_peak()
@@ -266,7 +266,8 @@ def run_ours(args):
             "gpu_launches": int(st["kernel_launches"]),
             "clocks": head["clocks"],
             "lanczos_iters_per_node": st["lanczos_iters"] / n, "fermi_iters": st["fermi_iters"],
-            "lambda_f": head["lam"],
+            "lambda_f": head["lam"], "defect_check": {"nodes_redone_fp64": int(st["defect_nodes"]),
+                                                      "ms": st["ms_defect"]},
         }
         if arms[0] in acc:
             res["accuracy"] = acc[arms[0]]
@@ -275,7 +276,8 @@ def run_ours(args):
             sub = {"step": steps_desc[arm], "value": nodes / f["dev"], "e2e": nodes / f["wall"],
                    "ms_per_step": f["dev"] * 1e3, "roofline": f["roofline"], "clocks": f["clocks"],
                    "lanczos_iters_per_node": f["st"]["lanczos_iters"] / n,
-                   "gpu_launches": int(f["st"]["kernel_launches"])}
+                   "gpu_launches": int(f["st"]["kernel_launches"]),
+                   "defect_check": {"nodes_redone_fp64": int(f["st"]["defect_nodes"]), "ms": f["st"]["ms_defect"]}}
             if arm in acc:
                 sub["accuracy"] = acc[arm]
             res[{"fp64": "fp64", "mixed": "fp32_mixed", "lq": "lanczos_quadrature"}[arm]] = sub

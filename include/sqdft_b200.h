@@ -115,6 +115,9 @@ typedef struct sqb_stats {
   int max_lanczos_iters;
   int kernel_launches;       /* kernels launched by the last SQ or forces call */
   double ms_vjp;             /* adjoint node kernel of the last sqb_moments_vjp */
+  double ms_defect;          /* defect check of a fast form in the last SQ step (its
+                                sensitivity kernel, FP64 redo and superseded Fermi solve) */
+  long long defect_nodes;    /* nodes the last SQ step's defect check redid in FP64 */
 } sqb_stats;
 
 /* Create a context on CUDA device `device` (cudaSetDevice).  Mirrors the
@@ -133,6 +136,18 @@ int sqb_set_precision(sqb_ctx *ctx, int precision);
  * reference's start vector and sqb_grid.lanczos_tol.  No counterpart in the
  * reference. */
 int sqb_set_mixed_lanczos(sqb_ctx *ctx, double tol, double checkerboard);
+/* Density budget of the fast forms' defect check (relative to max rho, e.g.
+ * 1e-6; default 0, the check off).  When a fast form's Lanczos stop is
+ * looser than sqb_grid.lanczos_tol, sqb_spectral_quadrature evaluates every
+ * node's density at bounds moved by 4x the stop at either end, from the
+ * node's own moments (exact re-expansion of the Chebyshev polynomials, no
+ * matvec); nodes that move by more than half the budget are redone by the
+ * FP64 parity path and the Fermi level is solved again (the count is in
+ * sqb_stats.defect_nodes).  The 4x widening is conservative: where the
+ * looser stop already meets the budget it still redoes a share of the nodes
+ * (17% at npl 96, 40% of the step's time), hence opt-in.  No counterpart in
+ * the reference. */
+int sqb_set_defect_check(sqb_ctx *ctx, double budget);
 int sqb_set_allreduce(sqb_ctx *ctx, sqb_allreduce_fn fn, void *user);
 /* Launch shape of the node kernel: persistent CTAs per SM, and the layout of
  * its plane loop: window columns per thread (1 or 2; 0 = automatic, one

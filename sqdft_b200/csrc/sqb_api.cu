@@ -26,6 +26,7 @@ struct sqb_ctx {
   cudaStream_t stream = nullptr;
   int precision = SQB_FP64;
   double mixed_lanczos_tol = 0.0;  // Ha: the mixed path's Lanczos stop and margin (0: the grid's)
+  double defect_budget = 0.0;      // relative density budget of the fast forms' defect check (0: off)
   double mixed_lanczos_chk = 0.5;  // checkerboard weight of the mixed path's Lanczos start vector
   int cols = 0, ctas_per_sm = 1;
   int use_graph = 0;                       // replay the node-kernel sequence from a CUDA graph
@@ -71,6 +72,7 @@ struct sqb_ctx {
 
   double *d_xk = nullptr, *d_ctab = nullptr, *d_partial = nullptr, *d_result = nullptr;
   double *d_rho = nullptr, *d_ci = nullptr;
+  double *d_sens = nullptr;  // per-node density sensitivity of the defect check
   bool have_ci = false;
   double *d_fslots = nullptr, *d_f = nullptr;
   double *d_tmp = nullptr;
@@ -466,7 +468,7 @@ int sqb_destroy(sqb_ctx *c) {
                   c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
                   c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
-                  c->d_f, c->d_tmp};
+                  c->d_f, c->d_tmp, c->d_sens};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   drop_graph(c);
@@ -854,6 +856,87 @@ int sqb_density_energy(sqb_ctx *c, double lambda_f, double *rho, double *ci, dou
   return SQB_OK;
 }
 
+// Defect check of the fast forms (FP32-mixed, Lanczos quadrature) when their
+// Lanczos stop is looser than the grid's: the density of every node at
+// bounds moved by 4x the stop at either end is evaluated from the node's own
+// moments (re-expansion, bound_sens_kernel); nodes whose density moves by
+// more than half the budget times max rho are redone by the FP64 parity path
+// (the reference's bounds and moments), and the Fermi level is solved again.
+int defect_check(sqb_ctx *c, int scf_iter, double lambda_warm, double *lam) {
+  c->stats.defect_nodes = 0;
+  c->stats.ms_defect = 0.0;
+  const double tol_eff = std::max(c->g.lanczos_tol, c->mixed_lanczos_tol);
+  if (c->precision == SQB_FP64 || !(c->defect_budget > 0.0) || !(tol_eff > c->g.lanczos_tol)) return SQB_OK;
+  const int N = c->nnode;
+  if (!c->d_sens) CK(dalloc(&c->d_sens, (size_t)std::max(N, 1)));
+  const double ms_first_fermi = c->stats.ms_fermi;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  CK(launch_bound_sens(fermi_args(c), *lam, 4.0 * tol_eff, c->d_sens, c->d_rho, c->stream));
+  std::vector<double> sens(N), r0(N);
+  CK(cudaMemcpyAsync(sens.data(), c->d_sens, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(r0.data(), c->d_rho, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double mx = 0.0;
+  for (int i = 0; i < N; i++) mx = std::max(mx, r0[i]);
+  int rc = reduce(c, &mx, 1, SQB_MAX);
+  if (rc) return rc;
+  const double thr = 0.5 * c->defect_budget * mx;
+  std::vector<int> list;
+  for (int i = 0; i < N; i++)
+    if (!(sens[i] <= thr)) list.push_back(i);
+  double cnt = (double)list.size();
+  rc = reduce(c, &cnt, 1, SQB_SUM);
+  if (rc) return rc;
+  c->stats.defect_nodes = (long long)cnt;
+  c->stats.kernel_launches += 1;
+  if (cnt > 0) {
+    if (!list.empty()) {
+      rc = ensure_tmp(c, list.size() * sizeof(int));
+      if (rc) return rc;
+      int *d_list = reinterpret_cast<int *>(c->d_tmp);
+      CK(cudaMemcpyAsync(d_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+      NodeArgs a;
+      fill_node_args(c, a);
+      a.mode = MODE_SQ;
+      a.mixed = 0;  // the FP64 parity path
+      a.lq = 0;
+      a.lz_chk = 0.0;
+      a.lanczos_tol = c->g.lanczos_tol;
+      a.chi = c->d_chi;
+      a.zee = c->d_zee;
+      a.rho_pj = c->d_rho_pj;
+      a.lmin = c->d_lmin;
+      a.lmax = c->d_lmax;
+      a.lanczos_iters = c->d_iters;
+      rc = run_nodes(c, a, d_list, (int)list.size());
+      if (rc) return rc;
+      c->stats.kernel_launches += 1;
+    }
+    CK(launch_minmax(c->d_lmin, c->d_lmax, c->nnode, c->d_result, c->stream));
+    c->stats.kernel_launches += 1;
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  rc = read_status(c);
+  c->stats.ms_defect = elapsed(c);
+  if (rc || cnt == 0) return rc;
+  double mm[2];
+  CK(cudaMemcpy(mm, c->d_result, sizeof(mm), cudaMemcpyDeviceToHost));
+  rc = reduce(c, &mm[0], 1, SQB_MIN);
+  if (!rc) rc = reduce(c, &mm[1], 1, SQB_MAX);
+  if (rc) return rc;
+  c->lmin_all = mm[0];
+  c->lmax_all = mm[1];
+  rc = sqb_fermi_level(c, scf_iter, lambda_warm, lam, nullptr);
+  c->stats.ms_defect += ms_first_fermi;  // the first Fermi solve, now superseded
+  return rc;
+}
+
+int sqb_set_defect_check(sqb_ctx *c, double budget) {
+  if (!c || !(budget >= 0.0) || !std::isfinite(budget)) return SQB_ERR_ARG;
+  c->defect_budget = budget;
+  return SQB_OK;
+}
+
 int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *rho, double *rho_pj, double *ci,
                             double *chi, double *zee, double *ebs, double *eent) {
   if (!c || !lambda_f) return SQB_ERR_ARG;
@@ -862,6 +945,14 @@ int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *
   double lam = 0.0;
   rc = sqb_fermi_level(c, scf_iter, *lambda_f, &lam, nullptr);
   if (rc) return rc;
+  rc = defect_check(c, scf_iter, *lambda_f, &lam);
+  if (rc) return rc;
+  if (c->stats.defect_nodes > 0) {  // the redone nodes' bounds and moments
+    const size_t N = c->nnode, K = c->g.npl + 1;
+    if (chi) CK(cudaMemcpy(chi, c->d_chi, N * sizeof(double), cudaMemcpyDeviceToHost));
+    if (zee) CK(cudaMemcpy(zee, c->d_zee, N * sizeof(double), cudaMemcpyDeviceToHost));
+    if (rho_pj) CK(cudaMemcpy(rho_pj, c->d_rho_pj, N * K * sizeof(double), cudaMemcpyDeviceToHost));
+  }
   *lambda_f = lam;
   return sqb_density_energy(c, lam, rho, ci, ebs, eent);
 }

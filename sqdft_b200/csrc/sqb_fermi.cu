@@ -90,6 +90,79 @@ __global__ void __launch_bounds__(FTHREADS) ne_kernel(FermiArgs a, double lambda
   }
 }
 
+// Density of a node at bounds (chi', zee') from its moments at (chi, zee).
+// T_j((H - chi')/zee') = T_j(al Ht + be) with Ht = (H - chi)/zee, al = zee/zee',
+// be = (chi - chi')/zee', is a degree-j polynomial in Ht: its coefficients P_j
+// in the T_m(Ht) follow from P_j+1 = 2 (al X + be) P_j - P_j-1, X the product
+// by x in the Chebyshev basis (x T_0 = T_1, x T_m = (T_m+1 + T_m-1)/2), so the
+// moments at the new bounds are P_j . mu, exactly, with no new matvec.  The
+// density is then |2 sum_j c'_j mu'_j| with the coefficients of sq.cpp:1230-1259
+// on the new interval (sq.cpp:743-797).  One warp; buffers in w: 4K doubles.
+__device__ double rho_at_bounds(const FermiArgs &a, const double *mu, double chi, double zee, double chi2,
+                                double zee2, double lambda, const double *ctab, double *w) {
+  const int K = a.npl + 1, lane = threadIdx.x & 31;
+  double *pm = w, *pc = w + K, *pn = w + 2 * K, *mu2 = w + 3 * K;
+  const double al = zee / zee2, be = (chi - chi2) / zee2;
+  for (int m = lane; m < K; m += 32) {
+    pm[m] = m == 0 ? 1.0 : 0.0;
+    pc[m] = m == 0 ? be : (m == 1 ? al : 0.0);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    mu2[0] = mu[0];
+    mu2[1] = al * mu[1] + be * mu[0];
+  }
+  for (int j = 1; j < a.npl; j++) {
+    double acc = 0.0;
+    for (int m = lane; m < K; m += 32) {
+      const double up = m + 1 < K ? pc[m + 1] : 0.0;
+      const double xp = m == 0 ? 0.5 * up : (m == 1 ? pc[0] + 0.5 * up : 0.5 * (pc[m - 1] + up));
+      const double v = 2.0 * (al * xp + be * pc[m]) - pm[m];
+      pn[m] = v;
+      acc += v * mu[m];
+    }
+    acc = wsum(acc);
+    __syncwarp();
+    if (lane == 0) mu2[j + 1] = acc;
+    double *t = pm;
+    pm = pc;
+    pc = pn;
+    pn = t;
+    __syncwarp();
+  }
+  // Fermi-Dirac values on the new interval (pn is free), then 2 c' . mu'
+  const double lambda_fp = (lambda - chi2) / zee2, bet = a.bet0 * zee2;
+  for (int k = lane; k < K; k += 32) pn[k] = 1 / (1 + exp(bet * (a.xk[k] - lambda_fp)));
+  __syncwarp();
+  double r = 0.0;
+  for (int j = lane; j < K; j += 32) r += 2 * mu2[j] * cheb_coeff(pn, ctab, K, j);
+  r = wsum(r);
+  __syncwarp();
+  return fabs(r);
+}
+
+// Sensitivity of every node's density to its bounds: rho at bounds with the
+// lower end moved down by delta and, separately, the upper end moved up by
+// delta, against rho at the node's bounds; sens = the sum of the two changes.
+__global__ void __launch_bounds__(256) bound_sens_kernel(FermiArgs a, double lambda, double delta, double *sens,
+                                                         double *rho0) {
+  extern __shared__ __align__(16) double bsm[];
+  const int K = a.npl + 1;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double *buf = bsm + (size_t)w * 4 * K;
+  for (int node = blockIdx.x * nw + w; node < a.n_nodes; node += gridDim.x * nw) {
+    const double chi = a.chi[node], zee = a.zee[node];
+    const double *mu = a.rho_pj + (size_t)node * K;
+    const double r0 = rho_at_bounds(a, mu, chi, zee, chi, zee, lambda, a.ctab, buf);
+    const double rlo = rho_at_bounds(a, mu, chi, zee, chi - 0.5 * delta, zee + 0.5 * delta, lambda, a.ctab, buf);
+    const double rhi = rho_at_bounds(a, mu, chi, zee, chi + 0.5 * delta, zee + 0.5 * delta, lambda, a.ctab, buf);
+    if (lane == 0) {
+      sens[node] = fabs(rlo - r0) + fabs(rhi - r0);
+      rho0[node] = r0;
+    }
+  }
+}
+
 __global__ void sum_partials(const double *partial, int nblocks, int width, double *out) {
   __shared__ double red[32][2];
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -375,6 +448,19 @@ cudaError_t launch_density_energy(const FermiArgs &a, double lambda, cudaStream_
   const int nb = fermi_blocks(a.n_nodes);
   density_kernel<<<nb, FTHREADS, smem, s>>>(a, lambda, fits ? 1 : 0);
   sum_partials<<<1, 1024, 0, s>>>(a.partial, nb, 2, a.result);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bound_sens(const FermiArgs &a, double lambda, double delta, double *sens, double *rho0,
+                              cudaStream_t s) {
+  if (a.n_nodes <= 0) return cudaSuccess;
+  const size_t per_warp = (size_t)4 * (a.npl + 1) * sizeof(double);
+  int warps = 8;
+  while (warps > 1 && per_warp * warps > 48 * 1024) warps--;
+  if (per_warp * warps > 48 * 1024) return cudaErrorInvalidValue;
+  int blocks = (a.n_nodes + warps - 1) / warps;
+  if (blocks > 4096) blocks = 4096;
+  bound_sens_kernel<<<blocks, 32 * warps, per_warp * warps, s>>>(a, lambda, delta, sens, rho0);
   return cudaGetLastError();
 }
 

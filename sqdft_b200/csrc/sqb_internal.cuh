@@ -132,6 +132,8 @@ struct FermiArgs {
 };
 cudaError_t launch_ne_constraint(const FermiArgs &a, double lambda, int with_derivative, cudaStream_t s);
 cudaError_t launch_density_energy(const FermiArgs &a, double lambda, cudaStream_t s);
+cudaError_t launch_bound_sens(const FermiArgs &a, double lambda, double delta, double *sens, double *rho0,
+                              cudaStream_t s);
 int fermi_blocks(int n_nodes);
 
 // Force reduction and projector kernels.

@@ -37,7 +37,7 @@ EXPORTS = [
     "sqb_lanczos_moments", "sqb_ne_constraint", "sqb_fermi_level", "sqb_density_energy",
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
-    "sqb_set_graph", "sqb_set_mixed_lanczos",
+    "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check",
 ]
 
 
@@ -59,7 +59,7 @@ class SqbStats(C.Structure):
                 ("lanczos_iters", C.c_longlong), ("window_points", C.c_longlong), ("proj_points", C.c_longlong),
                 ("proj_points_cheb", C.c_longlong),
                 ("fermi_iters", C.c_int), ("max_lanczos_iters", C.c_int), ("kernel_launches", C.c_int),
-                ("ms_vjp", C.c_double)]
+                ("ms_vjp", C.c_double), ("ms_defect", C.c_double), ("defect_nodes", C.c_longlong)]
 
 
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, _dp, C.c_int, C.c_int, C.c_void_p)
@@ -86,6 +86,7 @@ def library() -> C.CDLL:
         lib.sqb_destroy.argtypes = [P]
         lib.sqb_set_precision.argtypes = [P, C.c_int]
         lib.sqb_set_mixed_lanczos.argtypes = [P, C.c_double, C.c_double]
+        lib.sqb_set_defect_check.argtypes = [P, C.c_double]
         lib.sqb_set_allreduce.argtypes = [P, ALLREDUCE_FN, C.c_void_p]
         lib.sqb_set_launch.argtypes = [P, C.c_int, C.c_int]
         lib.sqb_set_veff.argtypes = [P, _dp]
@@ -180,6 +181,10 @@ class Context:
         """Lanczos of the FP32-mixed path: stop and margin in Ha (0: the grid's
         lanczos_tol) and the checkerboard weight of the start vector."""
         _check(self.lib.sqb_set_mixed_lanczos(self.ptr, float(tol), float(checkerboard)), "sqb_set_mixed_lanczos")
+
+    def set_defect_check(self, budget: float = 1e-6):
+        """Turn on the fast forms' defect check with this density budget (0: off, the default)."""
+        _check(self.lib.sqb_set_defect_check(self.ptr, float(budget)), "sqb_set_defect_check")
 
     def set_launch(self, ctas_per_sm: int = 0, cols_per_thread: int = 0):
         _check(self.lib.sqb_set_launch(self.ptr, ctas_per_sm, cols_per_thread), "sqb_set_launch")

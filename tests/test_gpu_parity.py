@@ -260,3 +260,38 @@ def test_lanczos_quadrature_c2():
     assert rel <= 1e-6
     assert st[1]["matvecs"] <= 0.5 * st[0]["matvecs"]
     assert abs(outs[1]["lambda_f"] - outs[0]["lambda_f"]) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["lihs", "c1"])
+def test_defect_check_repairs_loose_stop(name):
+    """A 1e-3 Ha Lanczos stop misses the 1e-6 density budget at low order
+    (npl 16 LiH, npl 64 Al; 1e-4 to 1e-6 of max rho without the check).  The
+    defect check re-expands each node's moments to bounds moved by 4 mHa,
+    redoes in FP64 the nodes whose density moves by more than half the budget,
+    and brings both fast forms back within 1e-6 of the FP64 path."""
+    from sqdft_b200 import sq
+    from sqdft_b200.cases import load
+
+    case = load(name)
+
+    def run(prec, budget=1e-6):
+        with sq.Context(case, device=0, precision=prec) as ctx:
+            ctx.set_mixed_lanczos(1e-3)
+            ctx.set_defect_check(budget)
+            ctx.nonlocal_projectors()
+            out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+            return out, ctx.stats()
+
+    ref, _ = run(sq.SQB_FP64)
+    scale = np.abs(ref["rho"]).max()
+    for prec in (sq.SQB_FP32_MIXED, sq.SQB_FP64_LANCZOS_QUAD):
+        off, _ = run(prec, 0.0)
+        on, st = run(prec)
+        e_off = np.abs(off["rho"] - ref["rho"]).max() / scale
+        e_on = np.abs(on["rho"] - ref["rho"]).max() / scale
+        print(f"defect check {name} precision {prec}: rho {e_off:.2e} without, {e_on:.2e} with "
+              f"({st['defect_nodes']} of {case.n_nodes} nodes redone, {st['ms_defect']:.1f} ms)")
+        assert e_off > 1e-6
+        assert e_on <= 1e-6
+        assert 0 < st["defect_nodes"] <= case.n_nodes
+        assert abs(on["lambda_f"] - ref["lambda_f"]) <= 1e-6
