@@ -111,14 +111,14 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def algorithmic_bytes(stats, case, precision, lq=False):
+def algorithmic_bytes(stats, case, precision, lq=False, n_nodes=None):
     """Bytes per node-kernel launch by the roofline's accounting: per matvec
     step n_w (3 s_v + s_V) plus the projector tables of every atom whose ball
     meets the window, steps = Lanczos iterations + 1 + npl/2 per node.  Veff
     and the tables are FP64 in both paths; the Lanczos vectors (s_v) are FP32
     in the mixed path, the Chebyshev vectors FP64 in both."""
     nw = stats["window_points"]
-    n = case.n_nodes
+    n = case.n_nodes if n_nodes is None else n_nodes
     lz_steps = stats["lanczos_iters"] + n
     ch_steps = 0 if lq else n * (case.npl // 2)
     sv_lz = 8 if precision == 0 else 4
@@ -126,7 +126,45 @@ def algorithmic_bytes(stats, case, precision, lq=False):
     return (lz_steps * nw * (3 * sv_lz + 8) + proj_lz * 8) + (ch_steps * nw * 32 + stats["proj_points_cheb"] * 8)
 
 
+def run_sample(args):
+    """Node kernel alone on K evenly spaced nodes of a configuration (the
+    Lanczos bounds and Chebyshev moments of sq.cpp:530-661 for those nodes),
+    W untimed and S timed runs; prints one JSON line with the kernel time and
+    its algorithmic bytes.  For profiling a full-size configuration on a
+    subset of its nodes."""
+    import torch
+
+    from sqdft_b200 import sq
+    from sqdft_b200.cases import load as load_named
+
+    torch.cuda.set_device(0)
+    case = load_named(args.config)
+    prec = {"fp64": sq.SQB_FP64, "mixed": sq.SQB_FP32_MIXED, "lq": sq.SQB_FP64_LANCZOS_QUAD}[args.precision]
+    k = min(args.sample_nodes, case.n_nodes)
+    nodes = (np.arange(k, dtype=np.int64) * case.n_nodes // k).astype(np.int32)
+    with sq.Context(case, device=0, precision=prec) as ctx:
+        ctx.set_mixed_lanczos(args.mixed_lanczos_tol)
+        ctx.nonlocal_projectors()
+        for _ in range(args.warmup):
+            ctx.lanczos_moments_nodes(nodes)
+        ms = []
+        for _ in range(args.steps):
+            ctx.lanczos_moments_nodes(nodes)
+            st = ctx.stats()
+            ms.append(st["ms_lanczos_moments"])
+    kern = float(np.mean(ms)) * 1e-3
+    abytes = algorithmic_bytes(st, case, prec, lq=(args.precision == "lq"), n_nodes=k)
+    peak, peak_kind = hbm_peak()
+    print(json.dumps({"mode": "sample", "config": args.config, "precision": args.precision, "nodes": k,
+                      "kernel_ms": kern * 1e3, "nodes_per_s": k / kern,
+                      "lanczos_iters_per_node": st["lanczos_iters"] / k, "algorithmic_bytes": abytes,
+                      "achieved_gbs": abytes / kern / 1e9, "peak": peak, "peak_kind": peak_kind,
+                      "frac": abytes / kern / 1e9 / peak}), flush=True)
+
+
 def run_ours(args):
+    if args.precision != "all" and args.sample_nodes > 0:
+        return run_sample(args)
     import torch
     import torch.distributed as dist
 
@@ -369,6 +407,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sample-nodes", type=int, default=0,
+                    help="time the node kernel alone on this many nodes (needs --precision fp64|mixed|lq)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -33,7 +33,11 @@ extern "C" {
 #define SQB_ERR_NOT_BRACKETED 4    /* sq.cpp:1307-1311, Brent root not bracketed */
 #define SQB_ERR_FERMI_MAXITER 5    /* sq.cpp:1400-1401, Brent iteration limit */
 #define SQB_ERR_NEGATIVE_RHO 6     /* sq.cpp:764-765, rho < -1e-6 */
-#define SQB_ERR_LANCZOS_MAXITER 7  /* sq.cpp:1073-1074, Lanczos hit 500 iterations */
+#define SQB_ERR_LANCZOS_MAXITER 7  /* not returned: a node whose Lanczos hits 500
+                                      iterations keeps its last Ritz values and is
+                                      counted in sqb_stats.lanczos_maxiter_nodes, as
+                                      the reference prints and carries on
+                                      (sq.cpp:1073-1074) */
 #define SQB_ERR_DENOM_ZERO 8       /* nonlocal.cpp:163, zero KB denominator */
 #define SQB_ERR_SPLINE_RANGE 9     /* spline.cpp:17-22, radius outside the radial grid */
 #define SQB_ERR_CAPACITY 10        /* more projector atoms in one window than supported */
@@ -118,6 +122,8 @@ typedef struct sqb_stats {
   double ms_defect;          /* defect check of a fast form in the last SQ step (its
                                 sensitivity kernel, FP64 redo and superseded Fermi solve) */
   long long defect_nodes;    /* nodes the last SQ step's defect check redid in FP64 */
+  long long lanczos_maxiter_nodes; /* nodes of the last node kernel whose Lanczos stopped at
+                                      the 500-iteration cap (sq.cpp:1073-1074 prints them) */
 } sqb_stats;
 
 /* Create a context on CUDA device `device` (cudaSetDevice).  Mirrors the
@@ -204,6 +210,15 @@ int sqb_hsub_times_vec(sqb_ctx *ctx, int count, const int *nodes, const double *
 int sqb_lanczos_moments(sqb_ctx *ctx, double *chi, double *zee, double *rho_pj, int *lanczos_iters,
                         double *lambda_min, double *lambda_max);
 
+/* The per-node body of the node loop of ClenshawCurtisSpectralQuadrature
+ * (sq.cpp:530-661: Lanczos bounds and Chebyshev moments) for the `count`
+ * block nodes listed in `nodes` only.  Outputs are per listed node: chi, zee,
+ * lanczos_iters [count], rho_pj [count][npl+1]; any may be NULL.  The
+ * context's moments of the other nodes are left stale, so call
+ * sqb_lanczos_moments before sqb_fermi_level / sqb_density_energy. */
+int sqb_lanczos_moments_nodes(sqb_ctx *ctx, int count, const int *nodes, double *chi, double *zee, double *rho_pj,
+                              int *lanczos_iters);
+
 /* NeConstraint (sq.cpp:1183-1228) on the moments of the last
  * sqb_lanczos_moments call: 2 h^3 sum rho_pj.c(lambda) - N_e, reduced over
  * ranks through the allreduce hook. */
@@ -268,7 +283,13 @@ int sqb_moments_vjp(sqb_ctx *ctx, const double *g_mu, double *g_veff, double *g_
  * SQB_ERR_CAPACITY.  The first call on a device looks up the array's device
  * address for that device, so make it before any stream capture.  All calls
  * in the process share the array: calls that overlap on the GPU (other
- * threads or streams) race and must be serialised by the caller. */
+ * threads or streams) race and must be serialised by the caller.
+ * Ordering: the kernel runs on the context's private non-blocking stream,
+ * which first waits for the work queued so far on the legacy default stream
+ * (stream 0, where torch and most callers queue by default), so writes the
+ * caller queued there to the output arrays land before the kernel's.  Work
+ * the caller queued on any other stream must have finished (or the caller
+ * synchronises it) before the call. */
 int sqb_lanczos_moments_noalloc(sqb_ctx *ctx, int count, const int *nodes, double *d_chi, double *d_zee,
                                 double *d_rho_pj, int *d_lanczos_iters);
 

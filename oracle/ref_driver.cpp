@@ -18,7 +18,7 @@
 //                    (LanczosAlgorithm, sq.cpp:965, and the moment loop of
 //                    sq.cpp:564-655 over HsubTimesVec) on K nodes spread over
 //                    the block, on --threads T host threads; writes the
-//                    sampled chi, zee, rho_pj and the wall time
+//                    sampled chi, zee, rho_pj, the Veff block and the wall time
 // Writes <out_prefix>_in.sqc (inputs, incl. the reference's UdVtm tables) and
 // <out_prefix>_out.sqc (outputs and timings).
 #include <unistd.h>
@@ -214,6 +214,11 @@ int main(int argc, char **argv) {
     w.f64("sample_chi", chi.data(), {sample});
     w.f64("sample_zee", zee.data(), {sample});
     w.f64("sample_rho_pj", rpj.data(), {sample, SQ.npl + 1});
+    std::vector<double> vb((size_t)nnode);  // the Veff block the sample ran on
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) vb[((size_t)k * ny + j) * nx + i] = SQ.Veff[k + nl][j + nl][i + nl];
+    w.f64("veff_block", vb.data(), {nz, ny, nx});
     w.f64s("t_sample", secs);
     w.i32s("threads", threads);
     w.close();

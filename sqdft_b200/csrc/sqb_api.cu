@@ -79,6 +79,7 @@ struct sqb_ctx {
   size_t tmp_bytes = 0;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_order = nullptr;  // orders the no-alloc call after the caller's queued work
   sqb_stats stats{};
 };
 
@@ -118,7 +119,8 @@ int status_to_err(int st) {
   if (st & ST_FSLOTS) return SQB_ERR_CAPACITY;
   if (st & ST_SPLINE_RANGE) return SQB_ERR_SPLINE_RANGE;
   if (st & ST_NONFINITE) return SQB_ERR_NONFINITE;
-  if (st & ST_LANCZOS_MAXITER) return SQB_ERR_LANCZOS_MAXITER;
+  // ST_LANCZOS_MAXITER is a warning: the reference prints and carries on with
+  // the last Ritz values (sq.cpp:1073-1074); the nodes are counted in the stats.
   if (st & ST_WAIT_LIMIT) return SQB_ERR_CUDA;
   return SQB_OK;
 }
@@ -424,6 +426,7 @@ int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out) {
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&c->ev0));
   CK(cudaEventCreate(&c->ev1));
+  CK(cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming));
   CK(node_kernel_setup(c->n));
   const size_t N = c->nnode, K = g.npl + 1;
   CK(dalloc(&c->d_counter, 1));
@@ -474,6 +477,7 @@ int sqb_destroy(sqb_ctx *c) {
   drop_graph(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev_order) cudaEventDestroy(c->ev_order);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SQB_OK;
@@ -787,6 +791,11 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   }
   c->stats.lanczos_iters = sum;
   c->stats.max_lanczos_iters = mx;
+  long long capped = 0;
+  // (the quadrature form reports rows - 1 iterations, so its cap shows as 499)
+  const int cap = LANCZOS_MAX_ITER - (c->precision == SQB_FP64_LANCZOS_QUAD ? 1 : 0);
+  for (size_t i = 0; i < N; i++) capped += its[i] >= cap;
+  c->stats.lanczos_maxiter_nodes = capped;
   // passes: Lanczos 2 per iteration + 2, Chebyshev npl/2 (matvec passes only)
   c->stats.matvecs = sum + (long long)N + (c->precision == SQB_FP64_LANCZOS_QUAD ? 0LL : (long long)N * (c->g.npl / 2));
   c->stats.proj_points = (long long)pp[0];
@@ -799,6 +808,76 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   if (lambda_max) CK(cudaMemcpy(lambda_max, c->d_lmax, N * sizeof(double), cudaMemcpyDeviceToHost));
   c->have_moments = true;
   c->have_ci = false;
+  return SQB_OK;
+}
+
+int sqb_lanczos_moments_nodes(sqb_ctx *c, int count, const int *nodes, double *chi, double *zee, double *rho_pj,
+                              int *lanczos_iters) {
+  if (!c || count < 0 || (count > 0 && !nodes)) return SQB_ERR_ARG;
+  if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
+  if (count == 0) return SQB_OK;
+  for (int i = 0; i < count; i++)
+    if (nodes[i] < 0 || nodes[i] >= c->nnode) return SQB_ERR_ARG;
+  cudaSetDevice(c->device);
+  int rc = ensure_tmp(c, (size_t)count * sizeof(int));
+  if (rc) return rc;
+  int *d_list = reinterpret_cast<int *>(c->d_tmp);
+  CK(cudaMemcpyAsync(d_list, nodes, (size_t)count * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  NodeArgs a;
+  fill_node_args(c, a);
+  a.mode = MODE_SQ;
+  a.chi = c->d_chi;
+  a.zee = c->d_zee;
+  a.rho_pj = c->d_rho_pj;
+  a.lmin = c->d_lmin;
+  a.lmax = c->d_lmax;
+  a.lanczos_iters = c->d_iters;
+  c->stats.kernel_launches = 0;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  rc = run_nodes(c, a, d_list, count);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  c->stats.kernel_launches += 1;
+  rc = read_status(c);
+  c->stats.ms_lanczos_moments = elapsed(c);
+  // the per-node arrays now mix this call's nodes with older results
+  c->have_moments = false;
+  c->have_ci = false;
+  if (rc) return rc;
+  const size_t N = c->nnode, K = c->g.npl + 1;
+  std::vector<double> buf(N * K);
+  std::vector<int> its(N);
+  CK(cudaMemcpy(its.data(), c->d_iters, N * sizeof(int), cudaMemcpyDeviceToHost));
+  if (lanczos_iters)
+    for (int i = 0; i < count; i++) lanczos_iters[i] = its[nodes[i]];
+  long long capped = 0, sum = 0;
+  int mx = 0;
+  const int cap = LANCZOS_MAX_ITER - (c->precision == SQB_FP64_LANCZOS_QUAD ? 1 : 0);
+  for (int i = 0; i < count; i++) {
+    capped += its[nodes[i]] >= cap;
+    sum += its[nodes[i]];
+    mx = std::max(mx, its[nodes[i]]);
+  }
+  c->stats.lanczos_maxiter_nodes = capped;
+  c->stats.lanczos_iters = sum;
+  c->stats.max_lanczos_iters = mx;
+  c->stats.matvecs = sum + count + (c->precision == SQB_FP64_LANCZOS_QUAD ? 0LL : (long long)count * (c->g.npl / 2));
+  unsigned long long pp[2] = {0, 0};
+  CK(cudaMemcpy(pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
+  c->stats.proj_points = (long long)pp[0];
+  c->stats.proj_points_cheb = (long long)pp[1];
+  if (chi) {
+    CK(cudaMemcpy(buf.data(), c->d_chi, N * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < count; i++) chi[i] = buf[nodes[i]];
+  }
+  if (zee) {
+    CK(cudaMemcpy(buf.data(), c->d_zee, N * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < count; i++) zee[i] = buf[nodes[i]];
+  }
+  if (rho_pj) {
+    CK(cudaMemcpy(buf.data(), c->d_rho_pj, N * K * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < count; i++) std::memcpy(rho_pj + (size_t)i * K, &buf[(size_t)nodes[i] * K], K * sizeof(double));
+  }
   return SQB_OK;
 }
 
@@ -1280,6 +1359,12 @@ int sqb_lanczos_moments_noalloc(sqb_ctx *c, int count, const int *nodes, double 
   a.scratch_stride = stride;
   a.node_list = d_list;
   a.n_list = count;
+  // The outputs are the caller's device arrays: the work below runs on the
+  // context's own (non-blocking) stream, so it first waits for everything the
+  // caller queued on the legacy default stream (where torch and most callers
+  // queue by default) before it writes them.
+  CK(cudaEventRecord(c->ev_order, cudaStreamLegacy));
+  CK(cudaStreamWaitEvent(c->stream, c->ev_order, 0));
   // The array keeps the previous call's contents: the counter and status
   // start at zero, the node list is written; window slots need no clearing.
   CK(cudaMemsetAsync(base, 0, header, c->stream));

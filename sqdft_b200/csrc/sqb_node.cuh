@@ -1553,7 +1553,7 @@ __device__ void lanczos_quadrature(const NodeArgs &a, NodeShared &S, unsigned ch
       __syncwarp();
     }
   } else if (threadIdx.x == 0 && (long long)k > (long long)n * n * n) {
-    atomicOr(a.status, ST_LANCZOS_MAXITER);
+    atomicOr(a.status, ST_CAPACITY);  // the moment recurrence's k-vectors do not fit the window slots
   }
   __syncthreads();
 }

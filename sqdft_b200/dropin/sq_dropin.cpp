@@ -237,6 +237,9 @@ void ClenshawCurtisSpectralQuadrature(DS_SQ *p, int scf_iter) {
   p->Eent = eent;
   sqb_stats st;
   sqb_get_stats(g_ctx, &st, sizeof(st));
+  if (st.lanczos_maxiter_nodes > 0)  // sq.cpp:1073-1074: reported, the run goes on
+    std::printf("Error: Lanczos exceeded max_iter. count=%d on %lld nodes of rank %d \n", st.max_lanczos_iters,
+                st.lanczos_maxiter_nodes, rank);
   if (rank == 0) {
     std::printf("Lanczos took %d iterations (max over nodes, GPU). \n", st.max_lanczos_iters);
     std::printf("Brent's algorithm took %d iterations. \n", st.fermi_iters);

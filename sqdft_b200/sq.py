@@ -37,7 +37,7 @@ EXPORTS = [
     "sqb_lanczos_moments", "sqb_ne_constraint", "sqb_fermi_level", "sqb_density_energy",
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
-    "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check",
+    "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check", "sqb_lanczos_moments_nodes",
 ]
 
 
@@ -59,7 +59,8 @@ class SqbStats(C.Structure):
                 ("lanczos_iters", C.c_longlong), ("window_points", C.c_longlong), ("proj_points", C.c_longlong),
                 ("proj_points_cheb", C.c_longlong),
                 ("fermi_iters", C.c_int), ("max_lanczos_iters", C.c_int), ("kernel_launches", C.c_int),
-                ("ms_vjp", C.c_double), ("ms_defect", C.c_double), ("defect_nodes", C.c_longlong)]
+                ("ms_vjp", C.c_double), ("ms_defect", C.c_double), ("defect_nodes", C.c_longlong),
+                ("lanczos_maxiter_nodes", C.c_longlong)]
 
 
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, _dp, C.c_int, C.c_int, C.c_void_p)
@@ -95,6 +96,7 @@ def library() -> C.CDLL:
         lib.sqb_set_projectors.argtypes = [P, _dp]
         lib.sqb_hsub_times_vec.argtypes = [P, C.c_int, _ip, _dp, _dp]
         lib.sqb_lanczos_moments.argtypes = [P, _dp, _dp, _dp, _ip, _dp, _dp]
+        lib.sqb_lanczos_moments_nodes.argtypes = [P, C.c_int, _ip, _dp, _dp, _dp, _ip]
         lib.sqb_ne_constraint.argtypes = [P, C.c_double, _dp]
         lib.sqb_fermi_level.argtypes = [P, C.c_int, C.c_double, _dp, _ip]
         lib.sqb_density_energy.argtypes = [P, C.c_double, _dp, _dp, _dp, _dp]
@@ -272,6 +274,17 @@ class Context:
         _check(self.lib.sqb_lanczos_moments(self.ptr, _d(r["chi"]), _d(r["zee"]), _d(r["rho_pj"]),
                                             _i(r["lanczos_iters"]), _d(r["lmin"]), _d(r["lmax"])),
                "sqb_lanczos_moments")
+        return r
+
+    def lanczos_moments_nodes(self, nodes):
+        """Bounds and moments of the listed nodes only (arrays per listed node)."""
+        nodes = np.ascontiguousarray(nodes, np.int32)
+        k = len(nodes)
+        r = dict(chi=np.zeros(k), zee=np.zeros(k), rho_pj=np.zeros((k, self.case.npl + 1)),
+                 lanczos_iters=np.zeros(k, np.int32))
+        _check(self.lib.sqb_lanczos_moments_nodes(self.ptr, k, _i(nodes), _d(r["chi"]), _d(r["zee"]),
+                                                  _d(r["rho_pj"]), _i(r["lanczos_iters"])),
+               "sqb_lanczos_moments_nodes")
         return r
 
     def moments_at(self, chi: np.ndarray, zee: np.ndarray) -> np.ndarray:

@@ -8,10 +8,14 @@ tables UdVtm, grid parameters) and its outputs (rho, rho_pj, Ci, chi, zee,
 lambda_f, Ebs, Eent, nonlocal forces, and HsubTimesVec on seeded vectors).
 The radial pseudopotential tables are not stored.
 
-    python tests/golden/make_golden.py [system ...]
+    SQDFT_REFERENCE=/path/to/SQDFT python tests/golden/make_golden.py [system ...]
+
+SQDFT_REFERENCE (a checkout of the reference) is needed for the system ``al``,
+which reads the reference's own regression input.
 """
 from __future__ import annotations
 
+import os
 import subprocess
 import sys
 import tempfile
@@ -30,15 +34,22 @@ POT = ROOT / "oracle" / "_ref" / "pot"
 SYSTEMS = {"tiny": ["--hv", "3"], "lihs": ["--hv", "2"], "mid": ["--hv", "1"], "al": ["--no-forces"]}
 # The reference's own regression input tests/Al (4-atom Al, 10^3 grid, npl 28);
 # its published log (tests/Al/results_Al:82) gives the first-SCF Fermi level.
-REF_TESTS = Path("/root/reference/tests")
+
+
+def ref_tests() -> Path:
+    """tests/ of the reference checkout named by SQDFT_REFERENCE."""
+    ref = os.environ.get("SQDFT_REFERENCE")
+    if not ref or not (Path(ref) / "tests").is_dir():
+        raise SystemExit("set SQDFT_REFERENCE=/path/to/SQDFT (a checkout of the reference sources)")
+    return Path(ref) / "tests"
 
 
 def run_reference(name: str, extra: list[str], workdir: Path) -> tuple[dict, dict]:
     if name == "al":
         run = workdir / "al"
         run.mkdir()
-        (run / "al.input").write_text((REF_TESTS / "Al" / "test_Al.input").read_text())
-        atoms = (REF_TESTS / "Al" / "Al_eq.atoms").read_text().replace("../../pseudopotentials/", "")
+        (run / "al.input").write_text((ref_tests() / "Al" / "test_Al.input").read_text())
+        atoms = (ref_tests() / "Al" / "Al_eq.atoms").read_text().replace("../../pseudopotentials/", "")
         (run / "Al_eq.atoms").write_text(atoms)
     else:
         run = write_system(name, workdir)

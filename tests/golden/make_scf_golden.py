@@ -10,11 +10,12 @@ energy, the atomic forces and the Lanczos / Brent iteration counts.  The
 reference's own published log of that system (tests/Al/results_Al) is parsed
 the same way and stored beside it as ``published``.
 
-    python tests/golden/make_scf_golden.py
+    SQDFT_REFERENCE=/path/to/SQDFT python tests/golden/make_scf_golden.py
 """
 from __future__ import annotations
 
 import json
+import os
 import subprocess
 import sys
 import tempfile
@@ -28,7 +29,6 @@ from sqdft_b200.runlog import parse  # noqa: E402
 
 PROGRAM = ROOT / "oracle" / "_ref" / "sqdft_ref"
 POT = ROOT / "oracle" / "_ref" / "pot"
-PUBLISHED = Path("/root/reference/tests/Al/results_Al")
 
 
 def main() -> None:
@@ -38,7 +38,10 @@ def main() -> None:
             (run / pot.name).symlink_to(pot)
         out = subprocess.run([str(PROGRAM), "-name", "al_ref"], cwd=run, check=True, capture_output=True, text=True)
     golden = {"system": "al_ref", "program": "reference SQDFT built from source, 1 rank", **parse(out.stdout)}
-    golden["published"] = parse(PUBLISHED.read_text())
+    ref = os.environ.get("SQDFT_REFERENCE")
+    if not ref:
+        raise SystemExit("set SQDFT_REFERENCE=/path/to/SQDFT (a checkout of the reference sources)")
+    golden["published"] = parse((Path(ref) / "tests" / "Al" / "results_Al").read_text())
     dest = Path(__file__).parent / "al_ref_scf.json"
     dest.write_text(json.dumps(golden, indent=1) + "\n")
     print(f"{dest}: {len(golden['scf'])} SCF iterations, free energy {golden['free_energy']}")

@@ -56,3 +56,27 @@ def test_calls_out_of_order(golden):
         assert _err(lambda: ctx.lanczos_moments()) == 12  # projectors not set
         ctx.set_projectors(case.udvtm)
         assert _err(lambda: ctx.ne_constraint(0.1)) == 12  # no moments yet
+
+
+def test_lanczos_cap_is_a_counted_warning(golden):
+    """A Lanczos that cannot meet its tolerance (-1: |dl| > -1 always holds)
+    stops at the 500-iteration cap and carries on with its last Ritz values,
+    as the reference prints and carries on (sq.cpp:1073-1074): no error
+    status, the nodes are counted in the stats, and the bounds are the
+    oracle's after the same 500 iterations."""
+    from oracle.pyoracle import Oracle
+    from sqdft_b200 import sq
+
+    case, _ = golden("tiny")
+    capped = dataclasses.replace(case, lanczos_tol=-1.0)
+    nodes = np.array([0, 100, 511], np.int32)
+    with sq.Context(capped) as ctx:
+        ctx.set_projectors(case.udvtm)
+        m = ctx.lanczos_moments_nodes(nodes)
+        st = ctx.stats()
+    assert st["lanczos_maxiter_nodes"] == len(nodes)
+    assert np.all(m["lanczos_iters"] == 500)
+    ref = Oracle(capped, case.udvtm).lanczos_moments(nodes)
+    assert np.all(ref["lanczos_iters"][nodes] == 500)
+    assert np.abs(m["chi"] - ref["chi"][nodes]).max() <= 1e-9
+    assert np.abs(m["zee"] - ref["zee"][nodes]).max() <= 1e-9
