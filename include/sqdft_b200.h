@@ -124,6 +124,10 @@ typedef struct sqb_stats {
   long long defect_nodes;    /* nodes the last SQ step's defect check redid in FP64 */
   long long lanczos_maxiter_nodes; /* nodes of the last node kernel whose Lanczos stopped at
                                       the 500-iteration cap (sq.cpp:1073-1074 prints them) */
+  long long proj_points_window; /* as proj_points, with each ball clipped to the window (the
+                                   projector values a matvec reads) */
+  int node_kernel;           /* kernel of the last Lanczos + moments work: SQB_KERNEL_PLANE or
+                                SQB_KERNEL_SWEEP */
 } sqb_stats;
 
 /* Create a context on CUDA device `device` (cudaSetDevice).  Mirrors the
@@ -160,6 +164,23 @@ int sqb_set_allreduce(sqb_ctx *ctx, sqb_allreduce_fn fn, void *user);
  * column per thread when the window has at most 1024 columns), or -2 for the
  * row layout (a warp per two window rows, windows up to 32 wide). */
 int sqb_set_launch(sqb_ctx *ctx, int ctas_per_sm, int cols_per_thread);
+
+/* Kernel of the per-node Lanczos bounds and Chebyshev moments (the node loop
+ * of sq.cpp:530-661).  SQB_KERNEL_SWEEP: one plane sweep per matvec with the
+ * nonlocal term read from layered projector fields (per grid point, the
+ * projector of at most one ball in each of four layers of non-touching
+ * balls), the dot products accumulated along z; it covers systems whose
+ * balls split into four such layers (the FCC sublattices) with at most three
+ * projectors per type.  SQB_KERNEL_PLANE: the plane-streaming kernel with
+ * per-window box lists, any system.  SQB_KERNEL_AUTO (default): the sweep
+ * kernel where it covers the system.  Results agree to rounding.  The nonlocal
+ * forces, the adjoint, sqb_moments_at, sqb_hsub_times_vec and
+ * sqb_lanczos_moments_noalloc run the plane-streaming kernel.  No counterpart
+ * in the reference. */
+#define SQB_KERNEL_AUTO 0
+#define SQB_KERNEL_PLANE 1
+#define SQB_KERNEL_SWEEP 2
+int sqb_set_node_kernel(sqb_ctx *ctx, int kernel);
 
 /* CUDA-graph replay of the node-kernel sequence of sqb_lanczos_moments (and
  * so of the SQ step): work-queue and status resets, the persistent Lanczos +
@@ -271,8 +292,8 @@ int sqb_moments_vjp(sqb_ctx *ctx, const double *g_mu, double *g_veff, double *g_
  * that has to keep its memory footprint fixed.  No counterpart in the
  * reference.
  *
- * It runs the same node kernel as sqb_lanczos_moments for the `count` block
- * nodes listed in host array `nodes`, but the kernel's per-CTA window
+ * It runs the plane-streaming node kernel (SQB_KERNEL_PLANE) for the `count`
+ * block nodes listed in host array `nodes`, but the kernel's per-CTA window
  * vectors, its work-queue counter and status word live in one fixed device
  * array of SQB_NOALLOC_SCRATCH_BYTES compiled into the library, not in
  * memory from cudaMalloc.  Inputs are the context's resident Veff, atoms and

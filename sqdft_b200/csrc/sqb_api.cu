@@ -60,6 +60,16 @@ struct sqb_ctx {
   bool have_dtab = false;
   std::vector<double> h_rep_xyz;  // replica positions (for the derivative tables)
   long long stage_elems = 0;  // largest per-plane projector-slice footprint (values)
+  std::vector<int> h_rep_nn;  // [n_rep][4] nearest nodes and types (host copy)
+  // Sweep kernel (sqb_sweep.cuh) and its layered projector fields, built on
+  // first use after the projector tables are set.
+  int node_kernel = SQB_KERNEL_AUTO;
+  int lay_state = 0;  // 0 not built, 1 built and usable, -1 the sweep kernel does not cover this context
+  int n_gproj = 0, lay_pmax = 1, n_lrep = 0;
+  unsigned long long *d_lay_id = nullptr;
+  double *d_lay_chi = nullptr;
+  int4 *d_rep_box = nullptr;
+  int *d_rep_gpb = nullptr;
   bool have_atoms = false, have_proj = false;
 
   unsigned char *d_scratch = nullptr;
@@ -201,8 +211,184 @@ int run_nodes(sqb_ctx *c, NodeArgs &a, const int *d_list, int count) {
   a.n_list = count;
   CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
-  CK(cudaMemsetAsync(c->d_proj_points, 0, 2 * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->d_proj_points, 0, 3 * sizeof(unsigned long long), c->stream));
   CK(launch_node_kernel(a, grid, cols, c->stream));
+  return SQB_OK;
+}
+
+// Layered projector fields of the sweep kernel: the replica balls with
+// projectors, as boxes on the extended grid (the block with its nloc halo),
+// split greedily in replica order into layers whose balls neither overlap nor
+// touch along z (a gap of at least one plane where their x-y footprints
+// overlap).  The sweep kernel covers the context when four layers suffice,
+// every type has at most three projectors, the ids fit 16 bits and the
+// block's shared memory holds the kernel's working set; otherwise the
+// plane-streaming kernel runs.
+int ensure_layers(sqb_ctx *c) {
+  if (c->lay_state != 0) return SQB_OK;
+  c->lay_state = -1;
+  const int nl = c->g.nloc, E[3] = {c->ex, c->ey, c->ez};
+  struct Box {
+    int lo[3], hi[3], r, np, t;
+  };
+  std::vector<Box> boxes;
+  int pmax = 0, ngp = 0;
+  for (int r = 0; r < c->n_rep; r++) {
+    const int t = c->h_rep_nn[4 * r + 3], np = c->typ_nproj[t], nlc = c->typ_nlocc[t];
+    if (np == 0) continue;
+    Box b{};
+    bool in = true;
+    for (int d = 0; d < 3; d++) {
+      b.lo[d] = c->h_rep_nn[4 * r + d] - nlc - (c->g.pnode_s[d] - nl);
+      b.hi[d] = b.lo[d] + 2 * nlc;
+      in = in && b.hi[d] >= 0 && b.lo[d] < E[d];
+    }
+    if (!in) continue;
+    b.r = r;
+    b.np = np;
+    b.t = t;
+    boxes.push_back(b);
+    pmax = std::max(pmax, np);
+  }
+  std::vector<std::vector<int>> layers;
+  std::vector<int> layer_of(boxes.size());
+  for (size_t i = 0; i < boxes.size(); i++) {
+    const Box &b = boxes[i];
+    int k = 0;
+    for (; k < (int)layers.size(); k++) {
+      bool clash = false;
+      for (int j : layers[k]) {
+        const Box &o = boxes[j];
+        if (b.lo[0] <= o.hi[0] && o.lo[0] <= b.hi[0] && b.lo[1] <= o.hi[1] && o.lo[1] <= b.hi[1] &&
+            b.lo[2] <= o.hi[2] + 1 && o.lo[2] <= b.hi[2] + 1) {
+          clash = true;
+          break;
+        }
+      }
+      if (!clash) break;
+    }
+    if (k == (int)layers.size()) layers.emplace_back();
+    layers[k].push_back((int)i);
+    layer_of[i] = k;
+  }
+  std::vector<int4> box4(std::max<size_t>(boxes.size(), 1));
+  std::vector<int> gpb(std::max<size_t>(boxes.size(), 1));
+  for (size_t i = 0; i < boxes.size(); i++) {
+    const Box &b = boxes[i];
+    box4[i] = make_int4((b.lo[0] & 0xffff) | (b.hi[0] << 16), (b.lo[1] & 0xffff) | (b.hi[1] << 16),
+                        (b.lo[2] & 0xffff) | (b.hi[2] << 16), layer_of[i] | (b.np << 8) | (b.t << 16));
+    gpb[i] = ngp;
+    ngp += b.np;
+  }
+  const int pm = pmax <= 1 ? 1 : 3;
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  const bool usable = (int)layers.size() <= LAYERS && pmax <= LAY_PMAX && ngp + pm < 65535 &&
+                      sweep_threads(c->n) <= 1024 && sweep_smem(c->n, pm, ngp) <= (size_t)optin && c->n_typ < 256;
+  if (!usable) return SQB_OK;
+  const long long evol = (long long)c->ex * c->ey * c->ez;
+  c->n_gproj = ngp;
+  c->lay_pmax = pm;
+  c->n_lrep = (int)boxes.size();
+  CK(dalloc(&c->d_lay_id, (size_t)evol));
+  CK(dalloc(&c->d_lay_chi, (size_t)LAYERS * pm * evol));
+  CK(dalloc(&c->d_rep_box, box4.size()));
+  CK(dalloc(&c->d_rep_gpb, gpb.size()));
+  CK(cudaMemcpy(c->d_rep_box, box4.data(), box4.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_rep_gpb, gpb.data(), gpb.size() * sizeof(int), cudaMemcpyHostToDevice));
+  // the fill kernel indexes the padded tables by box: the offsets of the boxes' replicas
+  std::vector<long long> off_all(std::max(c->n_rep, 1));
+  CK(cudaMemcpy(off_all.data(), c->d_rep_off, off_all.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+  std::vector<long long> off(std::max<size_t>(boxes.size(), 1));
+  for (size_t i = 0; i < boxes.size(); i++) off[i] = off_all[boxes[i].r];
+  long long *d_off = nullptr;
+  CK(cudaMalloc((void **)&d_off, off.size() * sizeof(long long)));
+  CK(cudaMemcpy(d_off, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  const cudaError_t e = launch_fill_layers((int)boxes.size(), c->d_rep_box, c->d_rep_gpb, c->d_typ_nlocc, d_off,
+                                           c->d_tab64, c->ex, c->ey, c->ez, pm, ngp, c->d_lay_id, c->d_lay_chi,
+                                           c->stream);
+  const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+  cudaFree(d_off);
+  CK(e);
+  CK(e2);
+  c->lay_state = 1;
+  return SQB_OK;
+}
+
+// Whether the SQ node work of this context runs on the sweep kernel.
+int use_sweep(sqb_ctx *c, bool *yes) {
+  *yes = false;
+  if (c->node_kernel == SQB_KERNEL_PLANE) return SQB_OK;
+  int rc = ensure_layers(c);
+  if (rc) return rc;
+  if (c->lay_state != 1) return c->node_kernel == SQB_KERNEL_SWEEP ? SQB_ERR_UNSUPPORTED : SQB_OK;
+  *yes = true;
+  return SQB_OK;
+}
+
+// Lanczos bounds and Chebyshev moments (MODE_SQ) of `count` nodes of d_list
+// with the outputs of `a`, on the sweep kernel where it covers the context,
+// else on the plane-streaming node kernel.
+int run_sq_nodes(sqb_ctx *c, NodeArgs &a, const int *d_list, int count) {
+  bool sw = false;
+  int rc = use_sweep(c, &sw);
+  if (rc) return rc;
+  c->stats.node_kernel = sw ? SQB_KERNEL_SWEEP : SQB_KERNEL_PLANE;
+  if (!sw) return run_nodes(c, a, d_list, count);
+  int grid = c->sms;
+  if (grid > count) grid = count;
+  if (grid < 1) grid = 1;
+  const size_t nw = (size_t)c->n * c->n * c->n;
+  const size_t stride = ((3 * nw * sizeof(double)) + 255) & ~size_t(255);
+  if (c->scratch_bytes < stride * (size_t)grid) {
+    if (c->d_scratch) cudaFree(c->d_scratch);
+    c->d_scratch = nullptr;
+    c->scratch_bytes = 0;
+    CK(cudaMalloc((void **)&c->d_scratch, stride * (size_t)grid));
+    c->scratch_bytes = stride * (size_t)grid;
+  }
+  SweepArgs s;
+  std::memset(&s, 0, sizeof(s));
+  s.form = a.lq ? 2 : (a.mixed ? 1 : 0);
+  s.n = c->n;
+  s.nloc = c->g.nloc;
+  s.npl = c->g.npl;
+  for (int d = 0; d < 3; d++) s.np[d] = c->g.np[d];
+  s.ex = c->ex;
+  s.ey = c->ey;
+  s.evol = (long long)c->ex * c->ey * c->ez;
+  s.h3 = c->h3;
+  s.lanczos_tol = a.lanczos_tol;
+  s.lz_chk = a.lz_chk;
+  for (int k = 0; k <= FDN; k++) s.coeff_lap[k] = c->g.coeff_lap[k];
+  s.veff64 = c->d_veff64;
+  s.n_gproj = c->n_gproj;
+  s.pmax = c->lay_pmax;
+  s.lay_id = c->d_lay_id;
+  s.lay_chi = c->d_lay_chi;
+  s.n_rep = c->n_lrep;
+  s.rep_box = c->d_rep_box;
+  s.rep_gpb = c->d_rep_gpb;
+  s.typ_nlocc = c->d_typ_nlocc;
+  s.proj_denom = c->d_proj_denom;
+  s.node_list = d_list;
+  s.n_list = count;
+  s.counter = c->d_counter;
+  s.status = c->d_status;
+  s.scratch = c->d_scratch;
+  s.scratch_stride = stride;
+  s.nsweep = sweep_threads(c->n);
+  s.chi = a.chi;
+  s.zee = a.zee;
+  s.rho_pj = a.rho_pj;
+  s.lmin = a.lmin;
+  s.lmax = a.lmax;
+  s.lanczos_iters = a.lanczos_iters;
+  s.proj_points = c->d_proj_points;
+  CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->d_proj_points, 0, 3 * sizeof(unsigned long long), c->stream));
+  CK(launch_sweep(s, grid, c->stream));
   return SQB_OK;
 }
 
@@ -428,10 +614,11 @@ int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out) {
   CK(cudaEventCreate(&c->ev1));
   CK(cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming));
   CK(node_kernel_setup(c->n));
+  CK(sweep_setup(c->n));
   const size_t N = c->nnode, K = g.npl + 1;
   CK(dalloc(&c->d_counter, 1));
   CK(dalloc(&c->d_status, 1));
-  CK(dalloc(&c->d_proj_points, 2));
+  CK(dalloc(&c->d_proj_points, 3));
   CK(dalloc(&c->d_nodes, N));
   CK(dalloc(&c->d_iters, N));
   CK(dalloc(&c->d_chi, N));
@@ -466,7 +653,7 @@ int sqb_destroy(sqb_ctx *c) {
   if (!c) return SQB_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void *ptrs[] = {c->d_veff64, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
+  void *ptrs[] = {c->d_lay_id, c->d_lay_chi, c->d_rep_box, c->d_rep_gpb, c->d_veff64, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
                   c->d_typ_nlocc, c->d_typ_nproj, c->d_typ_lmax, c->d_typ_lloc, c->d_typ_size, c->d_proj_denom,
                   c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
@@ -566,6 +753,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
     else all_tables = false;
   }
   std::vector<int> nn((size_t)4 * std::max(n_rep, 1));
+  c->lay_state = 0;  // the layered fields follow the projector tables
   std::vector<long long> off(std::max(n_rep, 1)), off_ref(std::max(n_rep, 1));
   long long total = 0, total_pad = 0;
   for (int r = 0; r < n_rep; r++) {
@@ -634,6 +822,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
     CK(cudaStreamSynchronize(c->stream));
     c->stage_elems = fp;
   }
+  c->h_rep_nn = nn;
   c->have_atoms = true;
   c->have_dtab = false;
   drop_graph(c);
@@ -679,6 +868,7 @@ int sqb_nonlocal_projectors(sqb_ctx *c, double *udvtm_out) {
   }
   c->have_proj = true;
   c->have_moments = false;
+  c->lay_state = 0;
   return SQB_OK;
 }
 
@@ -697,6 +887,7 @@ int sqb_set_projectors(sqb_ctx *c, const double *udvtm) {
   }
   c->have_proj = true;
   c->have_moments = false;
+  c->lay_state = 0;
   return SQB_OK;
 }
 
@@ -747,7 +938,7 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
     // capture the sequence once its buffers exist (a plain run allocated them)
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    rc = run_nodes(c, a, c->d_nodes, c->nnode);
+    rc = run_sq_nodes(c, a, c->d_nodes, c->nnode);
     if (!rc && launch_minmax(c->d_lmin, c->d_lmax, c->nnode, c->d_result, c->stream) != cudaSuccess) rc = SQB_ERR_CUDA;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (!rc && e == cudaSuccess && cudaGraphInstantiate(&c->sq_graph, g, 0) != cudaSuccess) c->sq_graph = nullptr;
@@ -761,7 +952,7 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   if (c->use_graph && c->sq_graph) {
     CK(cudaGraphLaunch(c->sq_graph, c->stream));
   } else {
-    rc = run_nodes(c, a, c->d_nodes, c->nnode);
+    rc = run_sq_nodes(c, a, c->d_nodes, c->nnode);
     if (rc) return rc;
     CK(launch_minmax(c->d_lmin, c->d_lmax, c->nnode, c->d_result, c->stream));
     c->sq_graph_warm = 1;
@@ -781,7 +972,7 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   const size_t N = c->nnode, K = c->g.npl + 1;
   std::vector<int> its(N);
   CK(cudaMemcpy(its.data(), c->d_iters, N * sizeof(int), cudaMemcpyDeviceToHost));
-  unsigned long long pp[2] = {0, 0};
+  unsigned long long pp[3] = {0, 0, 0};
   CK(cudaMemcpy(pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
   long long sum = 0;
   int mx = 0;
@@ -800,6 +991,7 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   c->stats.matvecs = sum + (long long)N + (c->precision == SQB_FP64_LANCZOS_QUAD ? 0LL : (long long)N * (c->g.npl / 2));
   c->stats.proj_points = (long long)pp[0];
   c->stats.proj_points_cheb = (long long)pp[1];
+  c->stats.proj_points_window = (long long)pp[2];
   if (lanczos_iters) std::memcpy(lanczos_iters, its.data(), N * sizeof(int));
   if (chi) CK(cudaMemcpy(chi, c->d_chi, N * sizeof(double), cudaMemcpyDeviceToHost));
   if (zee) CK(cudaMemcpy(zee, c->d_zee, N * sizeof(double), cudaMemcpyDeviceToHost));
@@ -834,7 +1026,7 @@ int sqb_lanczos_moments_nodes(sqb_ctx *c, int count, const int *nodes, double *c
   a.lanczos_iters = c->d_iters;
   c->stats.kernel_launches = 0;
   CK(cudaEventRecord(c->ev0, c->stream));
-  rc = run_nodes(c, a, d_list, count);
+  rc = run_sq_nodes(c, a, d_list, count);
   if (rc) return rc;
   CK(cudaEventRecord(c->ev1, c->stream));
   c->stats.kernel_launches += 1;
@@ -862,10 +1054,11 @@ int sqb_lanczos_moments_nodes(sqb_ctx *c, int count, const int *nodes, double *c
   c->stats.lanczos_iters = sum;
   c->stats.max_lanczos_iters = mx;
   c->stats.matvecs = sum + count + (c->precision == SQB_FP64_LANCZOS_QUAD ? 0LL : (long long)count * (c->g.npl / 2));
-  unsigned long long pp[2] = {0, 0};
+  unsigned long long pp[3] = {0, 0, 0};
   CK(cudaMemcpy(pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
   c->stats.proj_points = (long long)pp[0];
   c->stats.proj_points_cheb = (long long)pp[1];
+  c->stats.proj_points_window = (long long)pp[2];
   if (chi) {
     CK(cudaMemcpy(buf.data(), c->d_chi, N * sizeof(double), cudaMemcpyDeviceToHost));
     for (int i = 0; i < count; i++) chi[i] = buf[nodes[i]];
@@ -987,7 +1180,7 @@ int defect_check(sqb_ctx *c, int scf_iter, double lambda_warm, double *lam) {
       a.lmin = c->d_lmin;
       a.lmax = c->d_lmax;
       a.lanczos_iters = c->d_iters;
-      rc = run_nodes(c, a, d_list, (int)list.size());
+      rc = run_sq_nodes(c, a, d_list, (int)list.size());
       if (rc) return rc;
       c->stats.kernel_launches += 1;
     }
@@ -1034,6 +1227,19 @@ int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *
   }
   *lambda_f = lam;
   return sqb_density_energy(c, lam, rho, ci, ebs, eent);
+}
+
+int sqb_set_node_kernel(sqb_ctx *c, int kernel) {
+  if (!c || kernel < SQB_KERNEL_AUTO || kernel > SQB_KERNEL_SWEEP) return SQB_ERR_ARG;
+  if (kernel == SQB_KERNEL_SWEEP && c->have_proj) {
+    cudaSetDevice(c->device);
+    const int rc = ensure_layers(c);
+    if (rc) return rc;
+    if (c->lay_state != 1) return SQB_ERR_UNSUPPORTED;
+  }
+  c->node_kernel = kernel;
+  drop_graph(c);
+  return SQB_OK;
 }
 
 int sqb_set_graph(sqb_ctx *c, int on) {

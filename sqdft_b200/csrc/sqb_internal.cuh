@@ -98,6 +98,63 @@ struct NodeArgs {
   unsigned long long *proj_points; // algorithmic projector-ball points touched
 };
 
+// Layered projector fields of the sweep kernel (sqb_sweep.cuh).  The replica
+// balls are split into LAYERS layers in which no two balls overlap (in the
+// periodic FCC systems the four simple-cubic sublattices), so every point of
+// the extended grid (the block with its nloc halo, the domain of every node
+// window) lies in at most one ball per layer.  Per point and layer the field
+// holds the global index of that ball's first projector (16 bits, four layers
+// in one 64-bit word; n_gproj where no ball covers the point) and the values
+// of its projectors there (zero elsewhere).
+constexpr int LAYERS = 4;
+constexpr int LAY_PMAX = 3;  // projectors per replica the fields carry (l <= 1)
+
+struct SweepArgs {
+  int form;  // 0: FP64 (the reference's Lanczos + Chebyshev moments); 1: FP32-mixed
+             // (FP32 Lanczos vectors, FP64 moments); 2: Lanczos quadrature
+  int n, nloc, npl;
+  int np[3];
+  int ex, ey;
+  long long evol;  // ex * ey * ez
+  double h3, lanczos_tol, lz_chk;
+  double coeff_lap[FDN + 1];
+  const double *veff64;
+  // layered projector fields
+  int n_gproj;                       // projector instances of all replicas; the empty id
+  int pmax;                          // projectors per layer slot (1 or 3)
+  const unsigned long long *lay_id;  // [evol]: four 16-bit projector bases
+  const double *lay_chi;             // [LAYERS][pmax][evol]
+  // replicas with projectors, for each node's box list
+  int n_rep;
+  const int4 *rep_box;  // [n_rep] {x0 | x1 << 16, y0 | y1 << 16, z0 | z1 << 16, layer | nproj << 8 | type << 16},
+                        // ball corners on the extended grid
+  const int *rep_gpb;   // [n_rep] global index of the replica's first projector
+  const int *typ_nlocc;
+  const double *proj_denom;  // [n_typ][MAXPROJ_TYPE]
+  // work queue and outputs (indexed by node id)
+  const int *node_list;
+  int n_list;
+  int *counter;
+  int *status;
+  unsigned char *scratch;
+  size_t scratch_stride;  // bytes per CTA: three window vectors (FP64)
+  int nsweep;             // threads of the block (a multiple of 32)
+  double *chi, *zee, *rho_pj, *lmin, *lmax;
+  int *lanczos_iters;
+  unsigned long long *proj_points;  // [3]: ball points x steps (all, Chebyshev only), ball-in-window points x steps
+};
+
+// Sweep kernel launchers (sqb_sweep.cu).
+int sweep_threads(int n);
+size_t sweep_smem(int n, int pmax, int n_gproj);
+cudaError_t sweep_setup(int n);
+cudaError_t launch_sweep(const SweepArgs &a, int grid, cudaStream_t s);
+// Layered fields from the padded projector tables: ids and values of every
+// replica's ball on the extended grid (fields zeroed / set empty first).
+cudaError_t launch_fill_layers(int n_rep, const int4 *rep_box, const int *rep_gpb, const int *typ_nlocc,
+                               const long long *rep_off, const double *tab64, int ex, int ey, int ez, int pmax,
+                               int n_gproj, unsigned long long *lay_id, double *lay_chi, cudaStream_t s);
+
 // Host-side launchers (sqb_node.cu).
 int node_kernel_threads(int n, int cols);
 cudaError_t launch_node_kernel(const NodeArgs &a, int grid, int cols, cudaStream_t s);

@@ -26,6 +26,7 @@ SQB_FP64 = 0
 SQB_FP32_MIXED = 1
 SQB_FP64_LANCZOS_QUAD = 2
 SQB_SUM, SQB_MIN, SQB_MAX = 0, 1, 2
+SQB_KERNEL_AUTO, SQB_KERNEL_PLANE, SQB_KERNEL_SWEEP = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -38,6 +39,7 @@ EXPORTS = [
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
     "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check", "sqb_lanczos_moments_nodes",
+    "sqb_set_node_kernel",
 ]
 
 
@@ -60,7 +62,8 @@ class SqbStats(C.Structure):
                 ("proj_points_cheb", C.c_longlong),
                 ("fermi_iters", C.c_int), ("max_lanczos_iters", C.c_int), ("kernel_launches", C.c_int),
                 ("ms_vjp", C.c_double), ("ms_defect", C.c_double), ("defect_nodes", C.c_longlong),
-                ("lanczos_maxiter_nodes", C.c_longlong)]
+                ("lanczos_maxiter_nodes", C.c_longlong), ("proj_points_window", C.c_longlong),
+                ("node_kernel", C.c_int)]
 
 
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, _dp, C.c_int, C.c_int, C.c_void_p)
@@ -107,6 +110,7 @@ def library() -> C.CDLL:
         lib.sqb_moments_at.argtypes = [P, _dp, _dp, _dp]
         lib.sqb_autotune.argtypes = [P, C.c_int, _ip, _dp]
         lib.sqb_set_graph.argtypes = [P, C.c_int]
+        lib.sqb_set_node_kernel.argtypes = [P, C.c_int]
         lib.sqb_moments_vjp.argtypes = [P, _dp, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
@@ -190,6 +194,10 @@ class Context:
 
     def set_launch(self, ctas_per_sm: int = 0, cols_per_thread: int = 0):
         _check(self.lib.sqb_set_launch(self.ptr, ctas_per_sm, cols_per_thread), "sqb_set_launch")
+
+    def set_node_kernel(self, kernel: int = SQB_KERNEL_AUTO):
+        """Kernel of the Lanczos bounds and moments: auto, plane-streaming or sweep."""
+        _check(self.lib.sqb_set_node_kernel(self.ptr, int(kernel)), "sqb_set_node_kernel")
 
     def set_graph(self, on: bool = True):
         _check(self.lib.sqb_set_graph(self.ptr, int(bool(on))), "sqb_set_graph")

@@ -295,3 +295,47 @@ def test_defect_check_repairs_loose_stop(name):
         assert e_on <= 1e-6
         assert 0 < st["defect_nodes"] <= case.n_nodes
         assert abs(on["lambda_f"] - ref["lambda_f"]) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["tiny", "lihs", "mid"])
+@pytest.mark.parametrize("precision", [0, 1, 2], ids=["fp64", "fp32_mixed", "lanczos_quad"])
+def test_sweep_kernel_matches_plane_kernel(golden, name, precision):
+    """The sweep kernel (layered projector fields, one plane sweep per matvec)
+    and the plane-streaming kernel give the same bounds, moments and Lanczos
+    counts in the FP64 forms (to rounding) and in the FP32-mixed form to FP32
+    rounding of its Lanczos vectors (bounds 1e-7, counts within one step); in
+    FP64 both match the reference."""
+    from sqdft_b200 import sq
+
+    case, ref = golden(name)
+    with _ctx(case, precision) as ctx:
+        ctx.set_node_kernel(sq.SQB_KERNEL_PLANE)
+        plane = ctx.lanczos_moments()
+        assert ctx.stats()["node_kernel"] == sq.SQB_KERNEL_PLANE
+        ctx.set_node_kernel(sq.SQB_KERNEL_SWEEP)
+        sweep = ctx.lanczos_moments()
+        st = ctx.stats()
+        assert st["node_kernel"] == sq.SQB_KERNEL_SWEEP
+    tol = 1e-7 if precision == 1 else 1e-11
+    if precision == 1:
+        assert np.abs(plane["lanczos_iters"] - sweep["lanczos_iters"]).max() <= 1
+    else:
+        assert np.array_equal(plane["lanczos_iters"], sweep["lanczos_iters"])
+    for k in ("chi", "zee"):
+        assert np.abs(plane[k] - sweep[k]).max() <= tol
+    scale = np.abs(plane["rho_pj"]).max()
+    assert np.abs(plane["rho_pj"] - sweep["rho_pj"]).max() <= tol * scale
+    if precision == 0:
+        assert np.abs(sweep["chi"] - ref["chi"]).max() <= 1e-10
+        assert np.abs(sweep["zee"] - ref["zee"]).max() <= 1e-10
+        assert np.abs(sweep["rho_pj"] - ref["rho_pj"]).max() <= 1e-10 * np.abs(ref["rho_pj"]).max()
+    assert st["proj_points_window"] <= st["proj_points"]
+
+
+def test_sweep_kernel_is_the_default_where_it_applies(golden):
+    from sqdft_b200 import sq
+
+    case, _ = golden("mid")
+    with _ctx(case) as ctx:
+        ctx.lanczos_moments()
+        assert ctx.stats()["node_kernel"] == sq.SQB_KERNEL_SWEEP
