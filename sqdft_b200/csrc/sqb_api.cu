@@ -283,7 +283,9 @@ int ensure_layers(sqb_ctx *c) {
   const int pm = pmax <= 1 ? 1 : 3;
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  const long long evol_all = (long long)c->ex * c->ey * c->ez;
   const bool usable = (int)layers.size() <= LAYERS && pmax <= LAY_PMAX && ngp + pm < 65535 &&
+                      evol_all * LAYERS * LAY_PMAX < (1LL << 31) &&
                       sweep_threads(c->n) <= 1024 && sweep_smem(c->n, pm, ngp) <= (size_t)optin && c->n_typ < 256;
   if (!usable) return SQB_OK;
   const long long evol = (long long)c->ex * c->ey * c->ez;
@@ -338,8 +340,7 @@ int run_sq_nodes(sqb_ctx *c, NodeArgs &a, const int *d_list, int count) {
   int grid = c->sms;
   if (grid > count) grid = count;
   if (grid < 1) grid = 1;
-  const size_t nw = (size_t)c->n * c->n * c->n;
-  const size_t stride = ((3 * nw * sizeof(double)) + 255) & ~size_t(255);
+  const size_t stride = sweep_scratch_bytes(c->n, c->lay_pmax);
   if (c->scratch_bytes < stride * (size_t)grid) {
     if (c->d_scratch) cudaFree(c->d_scratch);
     c->d_scratch = nullptr;

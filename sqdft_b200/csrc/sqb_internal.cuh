@@ -137,7 +137,7 @@ struct SweepArgs {
   int *counter;
   int *status;
   unsigned char *scratch;
-  size_t scratch_stride;  // bytes per CTA: three window vectors (FP64)
+  size_t scratch_stride;  // bytes per CTA: three window vectors (FP64), then the flush buffer
   int nsweep;             // threads of the block (a multiple of 32)
   double *chi, *zee, *rho_pj, *lmin, *lmax;
   int *lanczos_iters;
@@ -147,6 +147,7 @@ struct SweepArgs {
 // Sweep kernel launchers (sqb_sweep.cu).
 int sweep_threads(int n);
 size_t sweep_smem(int n, int pmax, int n_gproj);
+size_t sweep_scratch_bytes(int n, int pmax);  // scratch per CTA
 cudaError_t sweep_setup(int n);
 cudaError_t launch_sweep(const SweepArgs &a, int grid, cudaStream_t s);
 // Layered fields from the padded projector tables: ids and values of every

@@ -79,8 +79,14 @@ cudaError_t setup_pm(size_t smem) {
 int sweep_threads(int n) { return sweep::sweep_threads_of(n); }
 
 size_t sweep_smem(int n, int pmax, int n_gproj) {
-  return sweep::shared_fixed() + sweep::planes_bytes(n) + sweep::ring_bytes(sweep::sweep_threads_of(n), pmax) +
-         sweep::flush_bytes(n, pmax) + (((size_t)(n_gproj + pmax) * sizeof(double) + 127) & ~size_t(127));
+  const int nt = sweep::sweep_threads_of(n);
+  return sweep::shared_fixed() + sweep::planes_bytes(n) + sweep::ring_bytes(nt, pmax) + sweep::accw_bytes(nt, pmax) +
+         (((size_t)(n_gproj + pmax) * sizeof(double) + 127) & ~size_t(127));
+}
+
+size_t sweep_scratch_bytes(int n, int pmax) {
+  const size_t nw = (size_t)n * n * n;
+  return ((3 * nw + sweep::flush_doubles(n, pmax)) * sizeof(double) + 255) & ~size_t(255);
 }
 
 cudaError_t sweep_setup(int n) {

@@ -22,9 +22,11 @@
 //   * the dot products chi_J . w of the sweep's output w, which the next
 //     matvec needs, are accumulated per thread along z for each layer; when a
 //     column leaves a ball (the layer's id changes) the column's partial sum
-//     goes to a shared flush plane, and one warp sums each ball's columns in a
-//     fixed order once the ball's last plane is done: deterministic, and one
-//     warp reduction per ball per sweep instead of one per ball per plane.
+//     goes to the CTA's flush buffer in global memory, at the slot of (layer,
+//     the ball's last window plane, column), which no other ball shares; after
+//     the last plane every warp sums whole balls from it in a fixed order:
+//     deterministic, one reduction per ball per sweep, none inside the plane
+//     loop.
 // Lanczos keeps the reference's recurrence, start vector and convergence test
 // (sq.cpp:965-1092) with one sweep per step: the sweep forms the next
 // unnormalised Lanczos vector from the stored vectors while loading it, and
@@ -68,9 +70,6 @@ struct Shared {
   // local projector instances p < n_pi
   short pi_e[MAXP];
   int pi_g[MAXP];
-  // instances by the plane their ball's last window plane is: olist[z] .. olist[z+1]
-  int olist[MAXN + 1];
-  short ilist[MAXP];
   double p_nxt[MAXP];  // chi^T w of the sweep's output
   double p_in[MAXP];   // chi^T W of a Lanczos sweep's input (one projector per layer slot)
   double p_den[MAXP];
@@ -86,24 +85,25 @@ __host__ __device__ inline size_t planes_bytes(int n) {
   const int P = plane_pitch(n);
   return ((size_t)(2 * P * P + P + 8) * sizeof(double) + 127) & ~size_t(127);
 }
-// Lanczos sweeps of the one-projector fields also sum the dot products of
-// their input (the exact chi^T W_m, see lanczos) into a second plane set,
-// updated in place every plane (the column slots are the thread's own) and
-// cleared by the warp that reduces the ball; the layers keep a gap of at
-// least one plane between the balls of one layer, so a ball never starts in a
-// column in the plane right after the previous ball of its layer ended.
+// Lanczos sweeps of the one-projector fields also accumulate the dot products
+// of their input (the exact chi^T W_m, see lanczos), flushed into a second
+// set of the flush buffer.  The buffer (per CTA, after the three window
+// vectors in the scratch) holds [set][layer][projector][plane][column].
 __host__ __device__ constexpr bool input_dots(int pm) { return pm == 1; }
-__host__ __device__ inline size_t flush_bytes(int n, int pm) {
-  return ((size_t)(input_dots(pm) ? 2 : 1) * KL * pm * n * n * sizeof(double) + 127) & ~size_t(127);
+__host__ __device__ inline size_t flush_doubles(int n, int pm) {
+  return (size_t)(input_dots(pm) ? 2 : 1) * KL * pm * n * n * n;
 }
 __host__ __device__ inline size_t shared_fixed() { return (sizeof(Shared) + 127) & ~size_t(127); }
-// The threads' rings of the FDN planes behind (RSLOT slots, sized for FP64),
-// used with the one-projector fields; with three projectors per slot the
-// flush planes leave no room for them and the window stays in registers.
+// The threads' rings of the FDN planes behind (RSLOT slots, sized for FP64).
 constexpr int RSLOT = 8;
-__host__ __device__ constexpr bool uses_ring(int pm) { return pm == 1; }
+__host__ __device__ constexpr bool uses_ring(int pm) { return pm >= 1; }
 __host__ __device__ inline size_t ring_bytes(int nsweep, int pm) {
   return uses_ring(pm) ? (((size_t)RSLOT * RY * nsweep * sizeof(double) + 127) & ~size_t(127)) : 0;
+}
+// Lanczos sweeps' input-dot partials, one slot per (layer, row, thread): the
+// owning thread accumulates, flushes and clears its own slots.
+__host__ __device__ inline size_t accw_bytes(int nsweep, int pm) {
+  return input_dots(pm) ? (((size_t)KL * RY * nsweep * sizeof(double) + 127) & ~size_t(127)) : 0;
 }
 __host__ __device__ inline int sweep_threads_of(int n) {
   const int cols = n * ((n + RY - 1) / RY);
@@ -154,38 +154,23 @@ __device__ __forceinline__ T *slot(const SweepArgs &a, int k) {
 }
 
 // Sum of one projector instance's flushed column partials over its box's
-// columns (one warp, fixed order), into p_nxt; with IND also the input dots
-// from the second plane set (cleared as they are read), into p_in.
+// columns, at the slots of its ball's last window plane (one warp, fixed
+// order), into p_nxt; with IND also the input dots of the second set, into
+// p_in.  The loads of a pass are independent, so they overlap.
 template <int PM, bool IND>
-__device__ __forceinline__ void reduce_instance(const SweepArgs &a, Shared &S, double *fb, int p, int lane) {
+__device__ __forceinline__ void reduce_instance(const SweepArgs &a, Shared &S, const double *fb, int p, int lane) {
   const int e = S.pi_e[p], q = p - S.e_pb[e], k = S.e_k[e];
   const int n = a.n, n2 = n * n;
-  const int x0 = S.e_x0[e], x1 = S.e_x1[e], y0 = S.e_y0[e], y1 = S.e_y1[e];
-  const int bx = x1 - x0 + 1;
-  const double *f = fb + (size_t)(k * PM + q) * n2 + x0;
-  double *fw = fb + (size_t)(KL * PM + k * PM + q) * n2 + x0;
+  const int x0 = S.e_x0[e], y0 = S.e_y0[e];
+  const int bx = S.e_x1[e] - x0 + 1, by = S.e_y1[e] - y0 + 1, cnt = bx * by;
+  const double *f = fb + ((size_t)(k * PM + q) * n + S.e_z1[e]) * n2 + y0 * n + x0;
+  const double *fw = f + (size_t)KL * PM * n * n2;
   double s = 0.0, sw = 0.0;
-  if (bx <= 16) {
-    const int lr = lane >> 4, lx = lane & 15;
-    if (lx < bx) {
 #pragma unroll 4
-      for (int y = y0 + lr; y <= y1; y += 2) {
-        s += f[y * n + lx];
-        if constexpr (IND) {
-          sw += fw[y * n + lx];
-          fw[y * n + lx] = 0.0;
-        }
-      }
-    }
-  } else {
-    for (int y = y0; y <= y1; y++)
-      for (int x = lane; x < bx; x += 32) {
-        s += f[y * n + x];
-        if constexpr (IND) {
-          sw += fw[y * n + x];
-          fw[y * n + x] = 0.0;
-        }
-      }
+  for (int i = lane; i < cnt; i += 32) {
+    const int yy = i / bx, xx = i - yy * bx;
+    s += f[yy * n + xx];
+    if constexpr (IND) sw += fw[yy * n + xx];
   }
   s = warp_sum(s);
   if constexpr (IND) sw = warp_sum(sw);
@@ -216,15 +201,16 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   const bool tv = tid < n * nrow;
   const int x = tv ? tid % n : 0, yb = tv ? (tid / n) * RY : 0;
   const int nl = a.nloc, gc = (nl * n + nl) * n + nl;  // window index of the centre
-  const long long EP = (long long)a.ex * a.ey, EV = a.evol;
+  const int EP = a.ex * a.ey, EV = (int)a.evol;  // the extended grid fits 32-bit indices
   const unsigned dummy = (unsigned)a.n_gproj;
   const unsigned long long empty = 0x0001000100010001ull * (unsigned long long)dummy;  // no ball in any layer
   T *sm = reinterpret_cast<T *>(dyn);
   T *ring = reinterpret_cast<T *>(dyn + planes_bytes(n));
-  double *fb = reinterpret_cast<double *>(dyn + planes_bytes(n) + ring_bytes(NS, PM));
-  double *fbw = fb + (size_t)KL * PM * n2;  // IND: the input's partials, summed in place
+  double *accw = reinterpret_cast<double *>(dyn + planes_bytes(n) + ring_bytes(NS, PM));
   const double *pcur =
-      reinterpret_cast<const double *>(dyn + planes_bytes(n) + ring_bytes(NS, PM) + flush_bytes(n, PM));
+      reinterpret_cast<const double *>(dyn + planes_bytes(n) + ring_bytes(NS, PM) + accw_bytes(NS, PM));
+  double *fb = slot<double>(a, 3);                // flush buffer: [set][layer][projector][plane][column]
+  double *fbw = fb + (size_t)KL * PM * n * n2;  // IND: the input's set
   const double *veff = a.veff64;
   const unsigned long long *lid = a.lay_id;
   const double *lchi = a.lay_chi;
@@ -237,13 +223,13 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
 
   int y[RY], col[RY];
   bool ok[RY];
-  long long xb[RY];
+  int xb[RY];
 #pragma unroll
   for (int j = 0; j < RY; j++) {
     y[j] = yb + j;
     ok[j] = tv && y[j] < n;
     col[j] = ok[j] ? y[j] * n + x : 0;
-    xb[j] = ((long long)S.gk * a.ey + (S.gj + (ok[j] ? y[j] : 0))) * a.ex + S.gi + x;
+    xb[j] = (S.gk * a.ey + (S.gj + (ok[j] ? y[j] : 0))) * a.ex + S.gi + x;
   }
   // ring slot of (row j, plane zz): ring[((zz mod RSLOT) * RY + j) * NS + tid]
   auto rslot = [&](int j, int zz) -> T & { return ring[(((zz + RSLOT) & (RSLOT - 1)) * RY + j) * NS + tid]; };
@@ -278,12 +264,13 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   unsigned long long idc[RY], idn[RY];
   double chc[RY][KL][PM];
   double acd[RY][KL][PM];
+  // IND: the input's partial of (layer k, row j) lives in accw[(k RY + j) NS + tid]
   auto load_ids = [&](int j, int zz) -> unsigned long long {
     return (ok[j] && zz < n) ? __ldg(lid + xb[j] + zz * EP) : empty;
   };
   auto load_point = [&](int j, int zz) {
     if (!ok[j] || zz >= n) return;
-    const long long X = xb[j] + zz * EP;
+    const int X = xb[j] + zz * EP;
     if constexpr (STENCIL) ve[j] = __ldg(veff + X);
     if constexpr (SK == SK_CH) {
       if (!io.first) q1[j] = io.p1_delta ? (T)(zz * n2 + col[j] == gc ? 1.0 : 0.0) : io.p1[zz * n2 + col[j]];
@@ -291,12 +278,12 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
     if constexpr (CHR) {
 #pragma unroll
       for (int k = 0; k < KL; k++)
-        chc[j][k][0] = lay_of(idc[j], k) != dummy ? __ldg(lchi + (long long)k * EV + X) : 0.0;
+        chc[j][k][0] = lay_of(idc[j], k) != dummy ? __ldg(lchi + k * EV + X) : 0.0;
     }
   };
-  auto chi_at = [&](int j, int k, int q, long long X) -> double {
+  auto chi_at = [&](int j, int k, int q, int X) -> double {
     if constexpr (CHR) return chc[j][k][0];
-    else return lay_of(idc[j], k) != dummy ? __ldg(lchi + (long long)(k * PM + q) * EV + X) : 0.0;
+    else return lay_of(idc[j], k) != dummy ? __ldg(lchi + (k * PM + q) * EV + X) : 0.0;
   };
 
 #pragma unroll
@@ -304,9 +291,11 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
     ve[j] = 0.0;
     q1[j] = T(0);
 #pragma unroll
-    for (int k = 0; k < KL; k++)
+    for (int k = 0; k < KL; k++) {
+      if constexpr (IND) accw[(k * RY + j) * NS + tid] = 0.0;
 #pragma unroll
       for (int q = 0; q < PM; q++) acd[j][k][q] = chc[j][k][q] = 0.0;
+    }
     idc[j] = load_ids(j, 0);
     idn[j] = load_ids(j, 1);
     if constexpr (STENCIL) {
@@ -337,10 +326,6 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
         if (ok[j]) smz[(y[j] + FDN) * P + x + FDN] = fut[j][C];
     }
     bar_sweep(NS);
-    // balls whose last window plane was z - 1: their flushed partials are complete
-    if (z >= 1)
-      for (int i = S.olist[z - 1] + warp; i < S.olist[z]; i += nwarp)
-        reduce_instance<PM, IND>(a, S, fb, S.ilist[i], lane);
     if (tv) {
       double hv[RY], v[RY];
       if constexpr (STENCIL) {
@@ -366,7 +351,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
         }
 #pragma unroll
         for (int j = 0; j < RY; j++) {
-          const long long X = xb[j] + z * EP;
+          const int X = xb[j] + z * EP;
           double vnl = 0.0;
 #pragma unroll
           for (int k = 0; k < KL; k++) {
@@ -405,22 +390,30 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
         }
         if (g == gc) S.center_val = o;
         if (!isfinite(o)) atomicOr(a.status, ST_NONFINITE);
-        const long long X = xb[j] + z * EP;
+        const int X = xb[j] + z * EP;
 #pragma unroll
         for (int k = 0; k < KL; k++) {
 #pragma unroll
           for (int q = 0; q < PM; q++) acd[j][k][q] += chi_at(j, k, q, X) * o;
           if constexpr (IND) {
-            if (lay_of(idc[j], k) != dummy) fbw[(size_t)k * n2 + col[j]] += chi_at(j, k, 0, X) * v[j];
+            if (lay_of(idc[j], k) != dummy) accw[(k * RY + j) * NS + tid] += chi_at(j, k, 0, X) * v[j];
           }
-          // the column leaves this layer's ball after plane z: flush its partial
-          if (z + 1 < n && lay_of(idc[j] ^ idn[j], k) != 0u) {
+        }
+        // a column that leaves a layer's ball after plane z flushes its partial
+        // to the slot of (layer, z, column)
+        const unsigned long long chg = idc[j] ^ idn[j];
+        if (z + 1 < n && chg != 0ull) {
+#pragma unroll
+          for (int k = 0; k < KL; k++) {
+            if (lay_of(chg, k) == 0u) continue;
             if (lay_of(idc[j], k) != dummy) {
 #pragma unroll
-              for (int q = 0; q < PM; q++) fb[(size_t)(k * PM + q) * n2 + col[j]] = acd[j][k][q];
+              for (int q = 0; q < PM; q++) fb[((k * PM + q) * n + z) * n2 + col[j]] = acd[j][k][q];
+              if constexpr (IND) fbw[(k * n + z) * n2 + col[j]] = accw[(k * RY + j) * NS + tid];
             }
 #pragma unroll
             for (int q = 0; q < PM; q++) acd[j][k][q] = 0.0;
+            if constexpr (IND) accw[(k * RY + j) * NS + tid] = 0.0;
           }
         }
       }
@@ -440,24 +433,23 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
       }
     }
   }
-  // balls that end at the window's last plane: flush after every reduction of
-  // plane n - 2 is done (a ball of the same layer may start at n - 1 in a
-  // column whose previous ball ended at n - 2)
-  bar_sweep(NS);
+  // balls that end at the window's last plane: every layer's open partial (a
+  // layer with no ball there writes a zero no reduction reads); then every
+  // ball's columns are summed
   if (tv) {
 #pragma unroll
     for (int j = 0; j < RY; j++) {
       if (!ok[j]) continue;
-      // every layer's open partial; a layer with no ball at plane n - 1 writes
-      // a zero no reduction reads
 #pragma unroll
-      for (int k = 0; k < KL; k++)
+      for (int k = 0; k < KL; k++) {
 #pragma unroll
-        for (int q = 0; q < PM; q++) fb[(size_t)(k * PM + q) * n2 + col[j]] = acd[j][k][q];
+        for (int q = 0; q < PM; q++) fb[((k * PM + q) * n + n - 1) * n2 + col[j]] = acd[j][k][q];
+        if constexpr (IND) fbw[(k * n + n - 1) * n2 + col[j]] = accw[(k * RY + j) * NS + tid];
+      }
     }
   }
   bar_sweep(NS);
-  for (int i = S.olist[n - 1] + warp; i < S.olist[n]; i += nwarp) reduce_instance<PM, IND>(a, S, fb, S.ilist[i], lane);
+  for (int p = warp; p < S.n_pi; p += nwarp) reduce_instance<PM, IND>(a, S, fb, p, lane);
   bar_sweep(NS);
 }
 
@@ -593,8 +585,8 @@ __device__ void tridiag_extremes(Shared &S, int m) {
 }
 
 // The boxes of the replica balls meeting this node's window (the
-// intersection test of nonlocal.cpp:66-108), their projector instances, the
-// per-plane lists of instances whose ball ends there, and the denominators.
+// intersection test of nonlocal.cpp:66-108), their projector instances and
+// the denominators.
 __device__ void setup_node(const SweepArgs &a, Shared &S) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int n = a.n;
@@ -662,14 +654,6 @@ __device__ void setup_node(const SweepArgs &a, Shared &S) {
     }
     S.n_ent = ne;
     S.n_pi = pb;
-    // instances ordered by their ball's last window plane (counting sort)
-    for (int z = 0; z <= n; z++) S.olist[z] = 0;
-    for (int e = 0; e < ne; e++) S.olist[S.e_z1[e] + 1] += S.e_np[e];
-    for (int z = 0; z < n; z++) S.olist[z + 1] += S.olist[z];
-    int fill[MAXN];
-    for (int z = 0; z < n; z++) fill[z] = S.olist[z];
-    for (int e = 0; e < ne; e++)
-      for (int q = 0; q < S.e_np[e]; q++) S.ilist[fill[S.e_z1[e]]++] = (short)(S.e_pb[e] + q);
   }
   __syncthreads();
   for (int e = 0; e < S.n_ent; e++)
@@ -688,12 +672,12 @@ __device__ void setup_node(const SweepArgs &a, Shared &S) {
 // into the gather array.
 __device__ void centre_projections(const SweepArgs &a, Shared &S, double *pcur) {
   const int nl = a.nloc;
-  const long long X = ((long long)(S.gk + nl) * a.ey + (S.gj + nl)) * a.ex + S.gi + nl;
+  const int X = ((S.gk + nl) * a.ey + (S.gj + nl)) * a.ex + S.gi + nl;
   for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) {
     const int e = S.pi_e[p], q = p - S.e_pb[e], k = S.e_k[e];
     const bool in = S.e_x0[e] <= nl && nl <= S.e_x1[e] && S.e_y0[e] <= nl && nl <= S.e_y1[e] && S.e_z0[e] <= nl &&
                     nl <= S.e_z1[e];
-    const double c = in ? a.lay_chi[(long long)(k * a.pmax + q) * a.evol + X] : 0.0;
+    const double c = in ? a.lay_chi[(k * a.pmax + q) * (int)a.evol + X] : 0.0;
     S.pw_cur[p] = c;
     S.pw_prev[p] = 0.0;
     pcur[S.pi_g[p]] = c / S.p_den[p];
@@ -936,13 +920,8 @@ __global__ void __launch_bounds__(MAXT, 1) sweep_kernel(SweepArgs a) {
   Shared &S = *reinterpret_cast<Shared *>(smem);
   unsigned char *dyn = smem + shared_fixed();
   double *pcur =
-      reinterpret_cast<double *>(dyn + planes_bytes(a.n) + ring_bytes(a.nsweep, PM) + flush_bytes(a.n, PM));
+      reinterpret_cast<double *>(dyn + planes_bytes(a.n) + ring_bytes(a.nsweep, PM) + accw_bytes(a.nsweep, PM));
   for (int i = threadIdx.x; i < a.n_gproj + PM; i += blockDim.x) pcur[i] = 0.0;  // [n_gproj..]: the empty id
-  if constexpr (input_dots(PM)) {  // the in-place input-dot slots start (and are left) cleared
-    double *fbw = reinterpret_cast<double *>(dyn + planes_bytes(a.n) + ring_bytes(a.nsweep, PM)) +
-                  (size_t)KL * PM * a.n * a.n;
-    for (int i = threadIdx.x; i < KL * a.n * a.n; i += blockDim.x) fbw[i] = 0.0;
-  }
   for (;;) {
     if (threadIdx.x == 0) {
       const int q = atomicAdd(a.counter, 1);
