@@ -111,7 +111,7 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def algorithmic_bytes(stats, case, precision, lq=False, n_nodes=None):
+def algorithmic_bytes(stats, case, precision, lq=False, n_nodes=None, window=False):
     """Bytes per node-kernel launch by the roofline's accounting: per matvec
     step n_w (3 s_v + s_V) plus the projector tables of every atom whose ball
     meets the window, steps = Lanczos iterations + 1 + npl/2 per node.  Veff
@@ -122,8 +122,10 @@ def algorithmic_bytes(stats, case, precision, lq=False, n_nodes=None):
     lz_steps = stats["lanczos_iters"] + n
     ch_steps = 0 if lq else n * (case.npl // 2)
     sv_lz = 8 if precision == 0 else 4
-    proj_lz = stats["proj_points"] - stats["proj_points_cheb"]
-    return (lz_steps * nw * (3 * sv_lz + 8) + proj_lz * 8) + (ch_steps * nw * 32 + stats["proj_points_cheb"] * 8)
+    vectors = lz_steps * nw * (3 * sv_lz + 8) + ch_steps * nw * 32
+    if window:  # projector values of each ball clipped to the window (what a matvec reads)
+        return vectors + stats["proj_points_window"] * 8
+    return vectors + stats["proj_points"] * 8
 
 
 def run_sample(args):
@@ -218,10 +220,12 @@ def run_ours(args):
         return wall, dev_ms, st, lamv.value, ebs.value
 
     peak, peak_kind = hbm_peak()
+    # DRAM bytes per node matvec step of the node kernel, measured with ncu on
+    # a node sample of the configuration (profiles/sweep_kernel_traffic.md)
     traffic = {}
-    tr = ROOT / "profiles" / "node_kernel_traffic.json"
+    tr = ROOT / "profiles" / "sweep_kernel_traffic.json"
     if tr.exists():
-        traffic = json.loads(tr.read_text())
+        traffic = json.loads(tr.read_text()).get(args.config, {})
 
     def measure(arm, warmup, steps):
         """warmup untimed and steps timed SQ steps of one precision; max over ranks."""
@@ -242,6 +246,7 @@ def run_ours(args):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         wall, dev, kern = t.tolist()
         abytes = algorithmic_bytes(st, my, prec, lq=(arm == "lq"))
+        wbytes = algorithmic_bytes(st, my, prec, lq=(arm == "lq"), window=True)
         achieved = abytes / kern / 1e9
         steps_local = st["lanczos_iters"] + n + (0 if arm == "lq" else n * (my.npl // 2))
         per_step = traffic.get(arm)
@@ -250,7 +255,9 @@ def run_ours(args):
                     roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                               "frac": achieved / peak, "peak_kind": peak_kind,
                               "traffic": (per_step * steps_local) if per_step else None, "algorithmic_bytes": abytes,
-                              "kernel": "node_kernel", "kernel_ms": kern * 1e3})
+                              "frac_window": wbytes / kern / 1e9 / peak, "algorithmic_bytes_window": wbytes,
+                              "kernel": "sweep_kernel" if st["node_kernel"] == sq.SQB_KERNEL_SWEEP else "node_kernel",
+                              "kernel_ms": kern * 1e3})
 
     # the line's value: W untimed + K timed steps; the comparison arms: 1 + 1
     # (their kernels are already loaded), which keeps the timed work near a
@@ -279,6 +286,49 @@ def run_ours(args):
                 "ebs_diff_per_atom": abs(r["ebs"] - ref_ebs) / case.n_atm, "lanczos_tol": args.mixed_lanczos_tol}
 
     acc = {arm: accuracy_of(arm) for arm in arms if arm != "fp64"}
+
+    # nonlocal forces (ForcesNonLocal, forces.cpp:318-578) after the FP64 step,
+    # timed; with a fast form run too, its force error against FP64
+    forces = None
+    if "fp64" in res_arms and not args.no_forces:
+        # the context still holds the FP64 arm's last step (the last arm run)
+        f64 = ctx.forces_nonlocal()
+        st64 = ctx.stats()
+        t = torch.tensor([st64["ms_forces"]], dtype=torch.float64, device="cuda")
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        fms = float(t[0])
+        forces = {"step": "ForcesNonLocal after the FP64 SQ step (npl-step Chebyshev recursion of the density-matrix "
+                          "column per node, FD gradient, projector contraction)", "nodes_per_s": n * ws / (fms * 1e-3),
+                  "kernel_ms": fms, "max_abs_force": float(np.abs(f64).max()), "unit": "nodes/s"}
+        fast = arms[0] if arms[0] != "fp64" else None
+        if fast:
+            ctx.set_precision(prec_of[fast])
+            ctx.spectral_quadrature(1, case.lambda_f, outputs=False)
+            ff = ctx.forces_nonlocal()
+            t = torch.tensor([float(np.abs(ff - f64).max())], dtype=torch.float64, device="cuda")
+            if ws > 1:
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            forces[f"force_err_{fast}_vs_fp64"] = float(t[0])
+
+    # FP64 arm against the reference's own per-node outputs on a seeded node
+    # sample of this configuration (tests/golden/<config>_ref.npz, made by the
+    # reference compiled from its sources): bounds and moments
+    parity = None
+    gold = ROOT / "tests" / "golden" / f"{args.config}_ref.npz"
+    if "fp64" in res_arms and ws == 1 and gold.exists():
+        z = np.load(gold)
+        if "sample_nodes" in z.files and "sample_rho_pj" in z.files:
+            ctx.set_precision(sq.SQB_FP64)
+            m = ctx.lanczos_moments_nodes(z["sample_nodes"])
+            rchi = z["sample_chi"] if "sample_chi" in z.files else z["chi"][z["sample_nodes"]]
+            rzee = z["sample_zee"] if "sample_zee" in z.files else z["zee"][z["sample_nodes"]]
+            parity = {"nodes": int(len(z["sample_nodes"])), "chi_max_abs": float(np.abs(m["chi"] - rchi).max()),
+                      "zee_max_abs": float(np.abs(m["zee"] - rzee).max()),
+                      "rho_pj_max_rel": float(np.abs(m["rho_pj"] - z["sample_rho_pj"]).max()
+                                              / np.abs(z["sample_rho_pj"]).max()),
+                      "reference": f"tests/golden/{args.config}_ref.npz"}
+
     steps_desc = {
         "fp64": "FP64 SQ step (Lanczos bounds + Chebyshev moments + Fermi level + density), the parity path",
         "mixed": "FP32-mixed SQ step (FP32 Lanczos vectors from a checkerboard-weighted start, looser Lanczos stop; "
@@ -327,6 +377,10 @@ def run_ours(args):
             res[{"fp64": "fp64", "mixed": "fp32_mixed", "lq": "lanczos_quadrature"}[arm]] = sub
         if "fp64" in res_arms and arms[0] != "fp64":
             res["speedup_vs_fp64"] = res_arms["fp64"]["dev"] / head["dev"]
+        if parity:
+            res["fp64_parity_vs_reference"] = parity
+        if forces:
+            res["forces"] = forces
         if cpu:
             res["cpu_baseline"] = cpu
     ctx.close()
@@ -407,6 +461,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forces", action="store_true", help="skip the nonlocal-force timing")
     ap.add_argument("--sample-nodes", type=int, default=0,
                     help="time the node kernel alone on this many nodes (needs --precision fp64|mixed|lq)")
     args = ap.parse_args()
