@@ -180,7 +180,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     case = load_named(args.config)
     my = slab(case, rank, ws)
-    arms = {"all": ["lq", "mixed", "fp64"], "fp64": ["fp64"], "mixed": ["mixed"], "lq": ["lq"]}[args.precision]
+    arms = {"all": ["mixed", "lq", "fp64"], "fp64": ["fp64"], "mixed": ["mixed"], "lq": ["lq"]}[args.precision]
     prec_of = {"fp64": sq.SQB_FP64, "mixed": sq.SQB_FP32_MIXED, "lq": sq.SQB_FP64_LANCZOS_QUAD}
     first = prec_of[arms[0]]
 
@@ -221,7 +221,7 @@ def run_ours(args):
 
     peak, peak_kind = hbm_peak()
     # DRAM bytes per node matvec step of the node kernel, measured with ncu on
-    # a node sample of the configuration (profiles/sweep_kernel_traffic.md)
+    # a node sample of the configuration (profiles/sweep_kernel_c2_traffic.md)
     traffic = {}
     tr = ROOT / "profiles" / "sweep_kernel_traffic.json"
     if tr.exists():
