@@ -172,7 +172,7 @@ def run_ours(args):
 
     from sqdft_b200 import sq
     from sqdft_b200.cases import load as load_named
-    from sqdft_b200.dist import allreduce_fn, slab
+    from sqdft_b200.dist import allreduce_fn, slab, slab_indices
 
     rank, ws, local = dist_env()
     if ws > 1:
@@ -194,6 +194,19 @@ def run_ours(args):
     veff_host[...] = my.veff
     outs = dict(rho=pin((n,)), rho_pj=pin((n, K1)), Ci=pin((n, K1)), chi=pin((n,)), zee=pin((n,)))
     flush = torch.empty(256 * 2**20, dtype=torch.uint8, device="cuda")
+    if ws > 1:
+        # every step: rank 0 uploads the whole-grid Veff, NCCL broadcasts it,
+        # each rank gathers its slab with the Rcut halo on its GPU and hands it
+        # to the library (sqb_set_veff_device); after the step the ranks'
+        # densities are all-gathered and rank 0 reads the whole grid back
+        grid_host = pin(case.veff_block.shape)
+        grid_host[...] = case.veff_block
+        grid_dev = torch.empty(case.veff_block.shape, dtype=torch.float64, device="cuda")
+        _, _, kz, ky, kx = slab_indices(case, rank, ws)
+        kz_d, ky_d, kx_d = (torch.from_numpy(k).cuda() for k in (kz, ky, kx))
+        rho_dev = torch.empty(n, dtype=torch.float64, device="cuda")
+        rho_all = torch.empty(n * ws, dtype=torch.float64, device="cuda")
+        rho_all_host = torch.empty(n * ws, dtype=torch.float64).pin_memory()
 
     import ctypes as C
 
@@ -205,7 +218,14 @@ def run_ours(args):
         if ws > 1:
             dist.barrier()
         t0 = time.perf_counter()
-        ctx.set_veff(veff_host)
+        if ws > 1:
+            if rank == 0:
+                grid_dev.copy_(torch.from_numpy(grid_host), non_blocking=True)
+            dist.broadcast(grid_dev, src=0)
+            vslab = grid_dev.index_select(0, kz_d).index_select(1, ky_d).index_select(2, kx_d).contiguous()
+            ctx.set_veff_device(vslab.data_ptr())
+        else:
+            ctx.set_veff(veff_host)
         lamv = C.c_double(case.lambda_f)
         ebs, eent = C.c_double(), C.c_double()
         rc = ctx.lib.sqb_spectral_quadrature(ctx.ptr, 1, C.byref(lamv), dp(outs["rho"]), dp(outs["rho_pj"]),
@@ -213,6 +233,11 @@ def run_ours(args):
                                              C.byref(eent))
         if rc:
             raise sq.SQBError(rc, "sqb_spectral_quadrature")
+        if ws > 1:
+            rho_dev.copy_(torch.from_numpy(outs["rho"]))
+            dist.all_gather_into_tensor(rho_all, rho_dev)
+            if rank == 0:
+                rho_all_host.copy_(rho_all)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         st = ctx.stats()
@@ -291,6 +316,12 @@ def run_ours(args):
     # timed; with a fast form run too, its force error against FP64
     forces = None
     if "fp64" in res_arms and not args.no_forces:
+        def force_bytes(st, sv):
+            # per node and recursion step: t_k, t_k-1 read, t_k+1 written (sv
+            # bytes each), Veff, D read and written (FP64); plus the projector
+            # balls meeting the window
+            return n * my.npl * st["window_points"] * (3 * sv + 24) + st["proj_points"] * 8
+
         # the context still holds the FP64 arm's last step (the last arm run)
         f64 = ctx.forces_nonlocal()
         st64 = ctx.stats()
@@ -298,18 +329,26 @@ def run_ours(args):
         if ws > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         fms = float(t[0])
+        fb = force_bytes(st64, 8)
         forces = {"step": "ForcesNonLocal after the FP64 SQ step (npl-step Chebyshev recursion of the density-matrix "
                           "column per node, FD gradient, projector contraction)", "nodes_per_s": n * ws / (fms * 1e-3),
-                  "kernel_ms": fms, "max_abs_force": float(np.abs(f64).max()), "unit": "nodes/s"}
+                  "kernel_ms": fms, "max_abs_force": float(np.abs(f64).max()), "unit": "nodes/s",
+                  "kernel": "sweep_force_kernel" if st64["node_kernel"] == sq.SQB_KERNEL_SWEEP else "node_kernel",
+                  "roofline": {"bound": "hbm", "achieved": fb / (fms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                               "frac": fb / (fms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
+                               "algorithmic_bytes": fb}}
         fast = arms[0] if arms[0] != "fp64" else None
         if fast:
             ctx.set_precision(prec_of[fast])
             ctx.spectral_quadrature(1, case.lambda_f, outputs=False)
             ff = ctx.forces_nonlocal()
-            t = torch.tensor([float(np.abs(ff - f64).max())], dtype=torch.float64, device="cuda")
+            stf = ctx.stats()
+            t = torch.tensor([float(np.abs(ff - f64).max()), stf["ms_forces"]], dtype=torch.float64, device="cuda")
             if ws > 1:
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
             forces[f"force_err_{fast}_vs_fp64"] = float(t[0])
+            forces[f"{fast}"] = {"nodes_per_s": n * ws / (float(t[1]) * 1e-3), "kernel_ms": float(t[1]),
+                                 "recursion_vectors": "fp32" if fast == "mixed" else "fp64"}
 
     # FP64 arm against the reference's own per-node outputs on a seeded node
     # sample of this configuration (tests/golden/<config>_ref.npz, made by the
@@ -339,8 +378,12 @@ def run_ours(args):
     res = None
     if rank == 0:
         nodes = case.n_nodes
-        h2d = my.veff.nbytes * ws
-        d2h = sum(a.nbytes for a in outs.values()) * ws
+        if ws > 1:  # the whole-grid Veff to rank 0's GPU, each rank's rho up for the gather; outputs down
+            h2d = case.veff_block.nbytes + outs["rho"].nbytes * ws
+            d2h = sum(a.nbytes for a in outs.values()) * ws + outs["rho"].nbytes * ws
+        else:
+            h2d = my.veff.nbytes
+            d2h = sum(a.nbytes for a in outs.values())
         cpu = cpu_baseline(args) if (ws == 1 and not args.no_cpu) else None
         st = head["st"]
         res = {

@@ -206,6 +206,13 @@ int sqb_autotune(sqb_ctx *ctx, int sample, int *chosen, double *ms_out);
 /* Veff on the block with its Rcut halo: the state of DS_SQ::Veff after the
  * halo exchange of sq.cpp:400-492. */
 int sqb_set_veff(sqb_ctx *ctx, const double *veff_ext);
+/* sqb_set_veff from device memory of the context's device (the same layout),
+ * for callers that hold Veff on the GPU, e.g. after a broadcast of the
+ * whole-grid potential to every rank's GPU.  Ordered after the work queued on
+ * the legacy default stream; the buffer may be reused when it returns.  The
+ * values are not checked on the host: a non-finite Veff surfaces as
+ * SQB_ERR_NONFINITE from the next step. */
+int sqb_set_veff_device(sqb_ctx *ctx, const double *veff_ext_device);
 
 /* Atom types and the replica atoms whose rc-ball meets the block + Rcut
  * region (Replica_atoms_Rcut, initialize.cpp:1003-1196), type-major as

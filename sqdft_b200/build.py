@@ -21,7 +21,7 @@ LIB = BUILD / "libsqdft_b200.so"
 INCLUDE = HERE.parent / "include"
 
 SOURCES = ["sqb_api.cu", "sqb_node.cu", "sqb_node_forces.cu", "sqb_node_vjp.cu", "sqb_node_mixed.cu", "sqb_node_lq.cu",
-           "sqb_fermi.cu", "sqb_sweep.cu"]
+           "sqb_fermi.cu", "sqb_sweep.cu", "sqb_sweep_forces.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

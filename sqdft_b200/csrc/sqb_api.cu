@@ -70,6 +70,7 @@ struct sqb_ctx {
   double *d_lay_chi = nullptr;
   int4 *d_rep_box = nullptr;
   int *d_rep_gpb = nullptr;
+  int *d_rep_atom_l = nullptr;  // global atom of each replica of d_rep_box
   bool have_atoms = false, have_proj = false;
 
   unsigned char *d_scratch = nullptr;
@@ -298,6 +299,13 @@ int ensure_layers(sqb_ctx *c) {
   CK(dalloc(&c->d_rep_gpb, gpb.size()));
   CK(cudaMemcpy(c->d_rep_box, box4.data(), box4.size() * sizeof(int4), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_rep_gpb, gpb.data(), gpb.size() * sizeof(int), cudaMemcpyHostToDevice));
+  {
+    std::vector<int> atom_all(std::max(c->n_rep, 1)), atom_l(std::max<size_t>(boxes.size(), 1));
+    CK(cudaMemcpy(atom_all.data(), c->d_rep_atom, atom_all.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < boxes.size(); i++) atom_l[i] = atom_all[boxes[i].r];
+    CK(dalloc(&c->d_rep_atom_l, atom_l.size()));
+    CK(cudaMemcpy(c->d_rep_atom_l, atom_l.data(), atom_l.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
   // the fill kernel indexes the padded tables by box: the offsets of the boxes' replicas
   std::vector<long long> off_all(std::max(c->n_rep, 1));
   CK(cudaMemcpy(off_all.data(), c->d_rep_off, off_all.size() * sizeof(long long), cudaMemcpyDeviceToHost));
@@ -328,6 +336,54 @@ int use_sweep(sqb_ctx *c, bool *yes) {
   return SQB_OK;
 }
 
+// Sweep-kernel scratch for `grid` CTAs (grown on demand).
+int ensure_sweep_scratch(sqb_ctx *c, int grid, size_t *stride) {
+  *stride = sweep_scratch_bytes(c->n, c->lay_pmax);
+  if (c->scratch_bytes < *stride * (size_t)grid) {
+    if (c->d_scratch) cudaFree(c->d_scratch);
+    c->d_scratch = nullptr;
+    c->scratch_bytes = 0;
+    CK(cudaMalloc((void **)&c->d_scratch, *stride * (size_t)grid));
+    c->scratch_bytes = *stride * (size_t)grid;
+  }
+  return SQB_OK;
+}
+
+// The context's part of a sweep-kernel launch (grid, fields, replicas, queue).
+void fill_sweep_args(sqb_ctx *c, const int *d_list, int count, size_t stride, SweepArgs &s) {
+  std::memset(&s, 0, sizeof(s));
+  s.n = c->n;
+  s.nloc = c->g.nloc;
+  s.npl = c->g.npl;
+  for (int d = 0; d < 3; d++) s.np[d] = c->g.np[d];
+  s.ex = c->ex;
+  s.ey = c->ey;
+  s.evol = (long long)c->ex * c->ey * c->ez;
+  s.h3 = c->h3;
+  s.lanczos_tol = c->g.lanczos_tol;
+  for (int k = 0; k <= FDN; k++) s.coeff_lap[k] = c->g.coeff_lap[k];
+  for (int k = 0; k <= FDN; k++) s.coeff_grad[k] = c->g.coeff_grad[k];
+  s.veff64 = c->d_veff64;
+  s.n_gproj = c->n_gproj;
+  s.pmax = c->lay_pmax;
+  s.lay_id = c->d_lay_id;
+  s.lay_chi = c->d_lay_chi;
+  s.n_rep = c->n_lrep;
+  s.rep_box = c->d_rep_box;
+  s.rep_gpb = c->d_rep_gpb;
+  s.rep_atom = c->d_rep_atom_l;
+  s.typ_nlocc = c->d_typ_nlocc;
+  s.proj_denom = c->d_proj_denom;
+  s.node_list = d_list;
+  s.n_list = count;
+  s.counter = c->d_counter;
+  s.status = c->d_status;
+  s.scratch = c->d_scratch;
+  s.scratch_stride = stride;
+  s.nsweep = sweep_threads(c->n);
+  s.proj_points = c->d_proj_points;
+}
+
 // Lanczos bounds and Chebyshev moments (MODE_SQ) of `count` nodes of d_list
 // with the outputs of `a`, on the sweep kernel where it covers the context,
 // else on the plane-streaming node kernel.
@@ -340,52 +396,20 @@ int run_sq_nodes(sqb_ctx *c, NodeArgs &a, const int *d_list, int count) {
   int grid = c->sms;
   if (grid > count) grid = count;
   if (grid < 1) grid = 1;
-  const size_t stride = sweep_scratch_bytes(c->n, c->lay_pmax);
-  if (c->scratch_bytes < stride * (size_t)grid) {
-    if (c->d_scratch) cudaFree(c->d_scratch);
-    c->d_scratch = nullptr;
-    c->scratch_bytes = 0;
-    CK(cudaMalloc((void **)&c->d_scratch, stride * (size_t)grid));
-    c->scratch_bytes = stride * (size_t)grid;
-  }
+  size_t stride = 0;
+  rc = ensure_sweep_scratch(c, grid, &stride);
+  if (rc) return rc;
   SweepArgs s;
-  std::memset(&s, 0, sizeof(s));
+  fill_sweep_args(c, d_list, count, stride, s);
   s.form = a.lq ? 2 : (a.mixed ? 1 : 0);
-  s.n = c->n;
-  s.nloc = c->g.nloc;
-  s.npl = c->g.npl;
-  for (int d = 0; d < 3; d++) s.np[d] = c->g.np[d];
-  s.ex = c->ex;
-  s.ey = c->ey;
-  s.evol = (long long)c->ex * c->ey * c->ez;
-  s.h3 = c->h3;
   s.lanczos_tol = a.lanczos_tol;
   s.lz_chk = a.lz_chk;
-  for (int k = 0; k <= FDN; k++) s.coeff_lap[k] = c->g.coeff_lap[k];
-  s.veff64 = c->d_veff64;
-  s.n_gproj = c->n_gproj;
-  s.pmax = c->lay_pmax;
-  s.lay_id = c->d_lay_id;
-  s.lay_chi = c->d_lay_chi;
-  s.n_rep = c->n_lrep;
-  s.rep_box = c->d_rep_box;
-  s.rep_gpb = c->d_rep_gpb;
-  s.typ_nlocc = c->d_typ_nlocc;
-  s.proj_denom = c->d_proj_denom;
-  s.node_list = d_list;
-  s.n_list = count;
-  s.counter = c->d_counter;
-  s.status = c->d_status;
-  s.scratch = c->d_scratch;
-  s.scratch_stride = stride;
-  s.nsweep = sweep_threads(c->n);
   s.chi = a.chi;
   s.zee = a.zee;
   s.rho_pj = a.rho_pj;
   s.lmin = a.lmin;
   s.lmax = a.lmax;
   s.lanczos_iters = a.lanczos_iters;
-  s.proj_points = c->d_proj_points;
   CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->d_proj_points, 0, 3 * sizeof(unsigned long long), c->stream));
@@ -616,6 +640,7 @@ int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out) {
   CK(cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming));
   CK(node_kernel_setup(c->n));
   CK(sweep_setup(c->n));
+  CK(sweep_forces_setup(c->n));
   const size_t N = c->nnode, K = g.npl + 1;
   CK(dalloc(&c->d_counter, 1));
   CK(dalloc(&c->d_status, 1));
@@ -654,7 +679,7 @@ int sqb_destroy(sqb_ctx *c) {
   if (!c) return SQB_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void *ptrs[] = {c->d_lay_id, c->d_lay_chi, c->d_rep_box, c->d_rep_gpb, c->d_veff64, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
+  void *ptrs[] = {c->d_lay_id, c->d_lay_chi, c->d_rep_box, c->d_rep_gpb, c->d_rep_atom_l, c->d_veff64, c->d_rep_nn, c->d_rep_atom, c->d_rep_off, c->d_typ_tab,
                   c->d_typ_nlocc, c->d_typ_nproj, c->d_typ_lmax, c->d_typ_lloc, c->d_typ_size, c->d_proj_denom,
                   c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
@@ -714,6 +739,23 @@ int sqb_set_veff(sqb_ctx *c, const double *veff_ext) {
     if (!std::isfinite(veff_ext[i])) return SQB_ERR_NONFINITE;
   if (!c->d_veff64) CK(dalloc(&c->d_veff64, n));
   CK(cudaMemcpyAsync(c->d_veff64, veff_ext, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_veff = true;
+  c->have_moments = false;
+  return SQB_OK;
+}
+
+int sqb_set_veff_device(sqb_ctx *c, const double *veff_ext) {
+  if (!c || !veff_ext) return SQB_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)c->ex * c->ey * c->ez;
+  if (!c->d_veff64) CK(dalloc(&c->d_veff64, n));
+  // after the work the caller queued on the legacy default stream (which
+  // wrote the block), then a device copy; the caller may reuse its buffer
+  // once this returns
+  CK(cudaEventRecord(c->ev_order, cudaStreamLegacy));
+  CK(cudaStreamWaitEvent(c->stream, c->ev_order, 0));
+  CK(cudaMemcpyAsync(c->d_veff64, veff_ext, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_veff = true;
   c->have_moments = false;
@@ -1475,17 +1517,39 @@ int sqb_forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const 
   } else if (!c->have_ci) {
     return SQB_ERR_STATE;
   }
-  NodeArgs a;
-  fill_node_args(c, a);
-  a.mode = MODE_FORCES;
-  a.chi_in = c->d_chi;
-  a.zee_in = c->d_zee;
-  a.ci = c->d_ci;
-  a.fslots = c->d_fslots;
-  c->stats.kernel_launches = 0;
-  CK(cudaEventRecord(c->ev0, c->stream));
-  int rc = run_nodes(c, a, c->d_nodes, c->nnode);
+  bool sw = false;
+  int rc = use_sweep(c, &sw);
   if (rc) return rc;
+  c->stats.kernel_launches = 0;
+  c->stats.node_kernel = sw ? SQB_KERNEL_SWEEP : SQB_KERNEL_PLANE;
+  if (sw) {
+    const int grid = std::max(1, std::min(c->sms, c->nnode));
+    size_t stride = 0;
+    rc = ensure_sweep_scratch(c, grid, &stride);
+    if (rc) return rc;
+    SweepArgs s;
+    fill_sweep_args(c, c->d_nodes, c->nnode, stride, s);
+    s.chi = c->d_chi;
+    s.zee = c->d_zee;
+    s.ci = c->d_ci;
+    s.fslots = c->d_fslots;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
+    CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    CK(cudaMemsetAsync(c->d_proj_points, 0, 3 * sizeof(unsigned long long), c->stream));
+    CK(launch_sweep_forces(s, c->precision == SQB_FP32_MIXED, grid, c->stream));
+  } else {
+    NodeArgs a;
+    fill_node_args(c, a);
+    a.mode = MODE_FORCES;
+    a.chi_in = c->d_chi;
+    a.zee_in = c->d_zee;
+    a.ci = c->d_ci;
+    a.fslots = c->d_fslots;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    rc = run_nodes(c, a, c->d_nodes, c->nnode);
+    if (rc) return rc;
+  }
   CK(launch_force_reduce(c->d_fslots, c->nnode, c->n_atm, c->d_f, c->stream));
   CK(cudaEventRecord(c->ev1, c->stream));
   c->stats.kernel_launches += 2;
@@ -1493,6 +1557,13 @@ int sqb_forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const 
   c->stats.ms_forces = elapsed(c);
   if (rc) return rc;
   if (c->n_atm > 0) CK(cudaMemcpy(forces, c->d_f, (size_t)3 * c->n_atm * sizeof(double), cudaMemcpyDeviceToHost));
+  if (sw) {  // the projector points the pass touched (roofline accounting)
+    unsigned long long pp[3] = {0, 0, 0};
+    CK(cudaMemcpy(pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
+    c->stats.proj_points = (long long)pp[0];
+    c->stats.proj_points_cheb = (long long)pp[1];
+    c->stats.proj_points_window = (long long)pp[2];
+  }
   return reduce(c, forces, 3 * c->n_atm, SQB_SUM);
 }
 

@@ -141,6 +141,14 @@ struct SweepArgs {
   int nsweep;             // threads of the block (a multiple of 32)
   double *chi, *zee, *rho_pj, *lmin, *lmax;
   int *lanczos_iters;
+  // ForcesNonLocal (sweep_force_kernel): bounds in chi, zee (inputs), the
+  // Chebyshev coefficients Ci [node][npl+1], the FD gradient coefficients,
+  // the global atom of each replica of rep_box, force slots per listed node
+  // [n_list][FSLOTS][4] (atom, fx, fy, fz; atom -1 unused)
+  const double *ci;
+  double coeff_grad[FDN + 1];
+  const int *rep_atom;
+  double *fslots;
   unsigned long long *proj_points;  // [3]: ball points x steps (all, Chebyshev only), ball-in-window points x steps
 };
 
@@ -150,6 +158,10 @@ size_t sweep_smem(int n, int pmax, int n_gproj);
 size_t sweep_scratch_bytes(int n, int pmax);  // scratch per CTA
 cudaError_t sweep_setup(int n);
 cudaError_t launch_sweep(const SweepArgs &a, int grid, cudaStream_t s);
+// ForcesNonLocal on the sweep kernel (sqb_sweep_forces.cu); single: FP32
+// storage of the Chebyshev vectors (the FP32-mixed form), else FP64.
+cudaError_t sweep_forces_setup(int n);
+cudaError_t launch_sweep_forces(const SweepArgs &a, int single, int grid, cudaStream_t s);
 // Layered fields from the padded projector tables: ids and values of every
 // replica's ball on the extended grid (fields zeroed / set empty first).
 cudaError_t launch_fill_layers(int n_rep, const int4 *rep_box, const int *rep_gpb, const int *typ_nlocc,
@@ -190,9 +202,9 @@ struct FermiArgs {
 };
 cudaError_t launch_ne_constraint(const FermiArgs &a, double lambda, int with_derivative, cudaStream_t s);
 cudaError_t launch_density_energy(const FermiArgs &a, double lambda, cudaStream_t s);
+int fermi_blocks(int n_nodes);
 cudaError_t launch_bound_sens(const FermiArgs &a, double lambda, double delta, double *sens, double *rho0,
                               cudaStream_t s);
-int fermi_blocks(int n_nodes);
 
 // Force reduction and projector kernels.
 cudaError_t launch_force_reduce(const double *fslots, int n_list, int n_atm, double *f, cudaStream_t s);

@@ -47,7 +47,10 @@ namespace sweep {
 constexpr int KL = LAYERS;
 constexpr int RY = 2;  // window rows per thread
 
-enum : int { SK_ONES = 0, SK_LZF = 1, SK_CH = 2 };
+// Sweep kinds: the Lanczos start vector's projections only; a Lanczos step;
+// a Chebyshev step; a Chebyshev step that also accumulates the density-matrix
+// column D += c t_k+1 / h^3 (ForcesNonLocal).
+enum : int { SK_ONES = 0, SK_LZF = 1, SK_CH = 2, SK_FD = 3 };
 
 struct Shared {
   int node, qidx, gi, gj, gk;
@@ -56,6 +59,8 @@ struct Shared {
   double center_val;
   double scal[2];
   double red[32][2];
+  double red3[32][3];
+  double scal2[3];
   double aa[MAXL];
   double bb[MAXL];
   double eig[2], eprev[2];
@@ -67,6 +72,7 @@ struct Shared {
   unsigned char e_k[MAXE], e_np[MAXE], e_t[MAXE];
   short e_pb[MAXE];  // first local projector instance
   int e_gpb[MAXE];   // first global projector id
+  int e_atom[MAXE];  // global atom (force passes)
   // local projector instances p < n_pi
   short pi_e[MAXP];
   int pi_g[MAXP];
@@ -137,6 +143,8 @@ struct IO {
   int p1_delta = 0;        // CH: t_k-1 is e_c
   int first = 0;           // CH: t_1 = (H t_0 - chi t_0) / zee (no t_k-1 term)
   int dbl = 0;             // CH: accumulate <t_k+1, t_k+1> and <t_k+1, t_k> (doubling)
+  double *dacc = nullptr;  // FD: density-matrix column, FP64
+  double cd = 0.0, ce = 0.0;  // FD: D += t_k+1 cd / h^3 (first: D = e_c ce / h^3 + t_1 cd / h^3)
 };
 
 // Lanczos start vector at window index g: 1 + chk (-1)^(x+y+z); the window
@@ -190,6 +198,7 @@ template <typename T, int PM, int SK>
 __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned char *dyn, const IO<T> &io,
                                       double &acc0, double &acc1) {
   constexpr bool STENCIL = SK != SK_ONES;
+  constexpr bool CHEB = SK == SK_CH || SK == SK_FD;
   constexpr bool RING = uses_ring(PM);
   constexpr int F = RING ? FDN + 1 : 2 * FDN + 1;  // planes held in registers
   constexpr int C = RING ? 0 : FDN;                // register index of the centre
@@ -261,6 +270,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   // per-plane point data, loaded one plane ahead
   double ve[RY];
   T q1[RY];
+  double dq[RY];  // FD: D at the point, loaded one plane ahead
   unsigned long long idc[RY], idn[RY];
   double chc[RY][KL][PM];
   double acd[RY][KL][PM];
@@ -272,9 +282,10 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
     if (!ok[j] || zz >= n) return;
     const int X = xb[j] + zz * EP;
     if constexpr (STENCIL) ve[j] = __ldg(veff + X);
-    if constexpr (SK == SK_CH) {
+    if constexpr (CHEB) {
       if (!io.first) q1[j] = io.p1_delta ? (T)(zz * n2 + col[j] == gc ? 1.0 : 0.0) : io.p1[zz * n2 + col[j]];
     }
+    if constexpr (SK == SK_FD) dq[j] = io.first ? 0.0 : io.dacc[zz * n2 + col[j]];
     if constexpr (CHR) {
 #pragma unroll
       for (int k = 0; k < KL; k++)
@@ -290,6 +301,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   for (int j = 0; j < RY; j++) {
     ve[j] = 0.0;
     q1[j] = T(0);
+    dq[j] = 0.0;
 #pragma unroll
     for (int k = 0; k < KL; k++) {
       if constexpr (IND) accw[(k * RY + j) * NS + tid] = 0.0;
@@ -387,6 +399,10 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
             acc0 += o * o;
             acc1 += o * v[j];
           }
+          if constexpr (SK == SK_FD) {  // forces.cpp:414-456
+            if (io.first) io.dacc[g] = 0.0 + (g == gc ? 1.0 : 0.0) * io.ce / a.h3 + o * io.cd / a.h3;
+            else io.dacc[g] = dq[j] + o * io.cd / a.h3;
+          }
         }
         if (g == gc) S.center_val = o;
         if (!isfinite(o)) atomicOr(a.status, ST_NONFINITE);
@@ -454,7 +470,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
 }
 
 // Sum of two values over the block into S.scal (deterministic).
-__device__ void sweep_sum2(Shared &S, double v0, double v1, int NS) {
+static __device__ void sweep_sum2(Shared &S, double v0, double v1, int NS) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = NS >> 5;
   v0 = warp_sum(v0);
   v1 = warp_sum(v1);
@@ -479,7 +495,7 @@ __device__ void sweep_sum2(Shared &S, double v0, double v1, int NS) {
 // Sturm count: eigenvalues of the leading m x m tridiagonal (d, e) below x,
 // from the sign changes of the characteristic-polynomial sequence, rescaled
 // by exact powers of two to stay in range.
-__device__ int sturm_count(const double *d, const double *e, int m, double x) {
+static __device__ int sturm_count(const double *d, const double *e, int m, double x) {
   double p0 = 1.0, p1 = d[0] - x;
   int s_prev = 1, cnt = 0;
   int s1 = p1 > 0.0 ? 1 : (p1 < 0.0 ? -1 : -s_prev);
@@ -510,7 +526,7 @@ __device__ int sturm_count(const double *d, const double *e, int m, double x) {
 // evaluates a Sturm count at one of its 32 G points (G warps per group), so the
 // bracket shrinks (32 G + 1)-fold per round, from the Gershgorin interval to
 // four units in the last place.  All threads call it.
-__device__ void tridiag_extremes(Shared &S, int m) {
+static __device__ void tridiag_extremes(Shared &S, int m) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   const int G = nw / 2, N = 32 * G;
   const int g = warp < G ? 0 : (warp < 2 * G ? 1 : 2);
@@ -587,7 +603,7 @@ __device__ void tridiag_extremes(Shared &S, int m) {
 // The boxes of the replica balls meeting this node's window (the
 // intersection test of nonlocal.cpp:66-108), their projector instances and
 // the denominators.
-__device__ void setup_node(const SweepArgs &a, Shared &S) {
+static __device__ void setup_node(const SweepArgs &a, Shared &S) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int n = a.n;
   if (tid == 0) S.n_ent = 0;
@@ -633,6 +649,7 @@ __device__ void setup_node(const SweepArgs &a, Shared &S) {
         S.e_np[pos] = (unsigned char)((b.w >> 8) & 0xff);
         S.e_t[pos] = (unsigned char)((b.w >> 16) & 0xff);
         S.e_gpb[pos] = a.rep_gpb[r];
+        S.e_atom[pos] = a.rep_atom ? a.rep_atom[r] : -1;
       } else {
         atomicOr(a.status, ST_CAPACITY);
       }
@@ -670,7 +687,7 @@ __device__ void setup_node(const SweepArgs &a, Shared &S) {
 // chi^T e_c of every instance (the projector values at the window centre;
 // zero for balls that do not hold it) into pw_cur, and c = chi^T e_c / Denom
 // into the gather array.
-__device__ void centre_projections(const SweepArgs &a, Shared &S, double *pcur) {
+static __device__ void centre_projections(const SweepArgs &a, Shared &S, double *pcur) {
   const int nl = a.nloc;
   const int X = ((S.gk + nl) * a.ey + (S.gj + nl)) * a.ex + S.gi + nl;
   for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) {
@@ -686,12 +703,12 @@ __device__ void centre_projections(const SweepArgs &a, Shared &S, double *pcur) 
 }
 
 // c_J = chi_J^T w / Denom_J of the last sweep's output into the gather array.
-__device__ void rotate(Shared &S, double *pcur) {
+static __device__ void rotate(Shared &S, double *pcur) {
   for (int p = threadIdx.x; p < S.n_pi; p += blockDim.x) pcur[S.pi_g[p]] = S.p_nxt[p] / S.p_den[p];
   __syncthreads();
 }
 
-__device__ void count_proj_points(const SweepArgs &a, Shared &S, long long steps, int cheb) {
+static __device__ void count_proj_points(const SweepArgs &a, Shared &S, long long steps, int cheb) {
   if (threadIdx.x != 0 || a.proj_points == nullptr) return;
   unsigned long long full = 0, win = 0;
   for (int e = 0; e < S.n_ent; e++) {
@@ -880,9 +897,169 @@ __device__ void moments(const SweepArgs &a, Shared &S, unsigned char *dyn, doubl
   }
 }
 
+// Sum of three values over the block into S.scal2 (deterministic).
+static __device__ void sweep_sum3(Shared &S, double v0, double v1, double v2) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  v0 = warp_sum(v0);
+  v1 = warp_sum(v1);
+  v2 = warp_sum(v2);
+  if (lane == 0) {
+    S.red3[warp][0] = v0;
+    S.red3[warp][1] = v1;
+    S.red3[warp][2] = v2;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    double r0 = lane < nw ? S.red3[lane][0] : 0.0;
+    double r1 = lane < nw ? S.red3[lane][1] : 0.0;
+    double r2 = lane < nw ? S.red3[lane][2] : 0.0;
+    r0 = warp_sum(r0);
+    r1 = warp_sum(r1);
+    r2 = warp_sum(r2);
+    if (lane == 0) {
+      S.scal2[0] = r0;
+      S.scal2[1] = r1;
+      S.scal2[2] = r2;
+    }
+  }
+  __syncthreads();
+}
+
+// ForcesNonLocal for one node (forces.cpp:318-578): the density-matrix column
+// D = sum_k Ci_k T_k((H - chi)/zee) e_c / h^3 by the full npl-step Chebyshev
+// recursion (vectors in storage precision T, D in FP64, slot 2 of the
+// scratch), then, on each ball that holds the window centre, the FD gradient
+// of D (zero outside the window) contracted with the replica's projectors:
+// f = -4 h^3 sum_q (chi_q . grad D) chi_q(centre) / Denom_q, into the node's
+// force slots (atom, fx, fy, fz).
+template <typename T, int PM>
+__device__ void node_forces(const SweepArgs &a, Shared &S, unsigned char *dyn, double *pcur, double chi,
+                            double zee, const double *ci, double *fslot) {
+  T *B0 = slot<T>(a, 0), *B1 = slot<T>(a, 1);
+  double *D = slot<double>(a, 2);
+  double d0 = 0.0, d1 = 0.0;
+  centre_projections(a, S, pcur);
+  {  // t_1 = (H e_c - chi e_c) / zee; D = e_c Ci_0 / h^3 + t_1 Ci_1 / h^3
+    IO<T> io;
+    io.konst = 2;
+    io.first = 1;
+    io.out = B1;
+    io.ca = chi;
+    io.cb = zee;
+    io.dacc = D;
+    io.ce = ci[0];
+    io.cd = ci[1];
+    sweep<T, PM, SK_FD>(a, S, dyn, io, d0, d1);
+  }
+  __syncthreads();
+  rotate(S, pcur);
+  T *t0 = B0, *t1 = B1;
+  for (int nq = 2; nq <= a.npl; nq++) {  // t_nq = 2 (H - chi)/zee t_nq-1 - t_nq-2; D += t_nq Ci_nq / h^3
+    IO<T> io;
+    io.vin = t1;
+    io.p1 = t0;
+    io.p1_delta = nq == 2;  // t_0 = e_c
+    io.out = t0;
+    io.ca = chi;
+    io.cb = zee;
+    io.dacc = D;
+    io.cd = ci[nq];
+    sweep<T, PM, SK_FD>(a, S, dyn, io, d0, d1);
+    __syncthreads();
+    rotate(S, pcur);
+    T *tt = t0;
+    t0 = t1;
+    t1 = tt;
+  }
+  __threadfence_block();
+  __syncthreads();
+  const int n = a.n, nl = a.nloc, n2 = n * n, EV = (int)a.evol;
+  int slotc = 0;
+  for (int e = 0; e < S.n_ent; e++) {
+    if (nl < S.e_x0[e] || nl > S.e_x1[e] || nl < S.e_y0[e] || nl > S.e_y1[e] || nl < S.e_z0[e] || nl > S.e_z1[e])
+      continue;
+    const int x0 = S.e_x0[e], y0 = S.e_y0[e], z0 = S.e_z0[e];
+    const int bx = S.e_x1[e] - x0 + 1, by = S.e_y1[e] - y0 + 1, bz = S.e_z1[e] - z0 + 1, vol = bx * by * bz;
+    const int k = S.e_k[e];
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int q = 0; q < S.e_np[e]; q++) {
+      const double *U = a.lay_chi + (size_t)(k * PM + q) * EV;
+      double ax = 0.0, ay = 0.0, az = 0.0;
+      for (int i = threadIdx.x; i < vol; i += blockDim.x) {
+        const int x = x0 + i % bx, y = y0 + (i / bx) % by, z = z0 + i / (bx * by);
+        const int w = z * n2 + y * n + x;
+        double gx = 0.0, gy = 0.0, gz = 0.0;
+        for (int kk = 1; kk <= FDN; kk++) {
+          const double xm = x - kk >= 0 ? D[w - kk] : 0.0, xp = x + kk < n ? D[w + kk] : 0.0;
+          const double ym = y - kk >= 0 ? D[w - kk * n] : 0.0, yp = y + kk < n ? D[w + kk * n] : 0.0;
+          const double zm = z - kk >= 0 ? D[w - kk * n2] : 0.0, zp = z + kk < n ? D[w + kk * n2] : 0.0;
+          gx += (-xm + xp) * a.coeff_grad[kk];
+          gy += (-ym + yp) * a.coeff_grad[kk];
+          gz += (-zm + zp) * a.coeff_grad[kk];
+        }
+        const double u = U[((S.gk + z) * a.ey + (S.gj + y)) * a.ex + S.gi + x];
+        ax += u * gx;
+        ay += u * gy;
+        az += u * gz;
+      }
+      sweep_sum3(S, ax, ay, az);
+      const double uc = U[((S.gk + nl) * a.ey + (S.gj + nl)) * a.ex + S.gi + nl];
+      const double den = S.p_den[S.e_pb[e] + q];
+      fx += S.scal2[0] / den * uc;
+      fy += S.scal2[1] / den * uc;
+      fz += S.scal2[2] / den * uc;
+    }
+    if (threadIdx.x == 0) {
+      if (slotc < FSLOTS) {
+        double *o = fslot + 4 * slotc;
+        o[0] = (double)S.e_atom[e];
+        o[1] = -4 * fx * a.h3;
+        o[2] = -4 * fy * a.h3;
+        o[3] = -4 * fz * a.h3;
+      } else {
+        atomicOr(a.status, ST_FSLOTS);
+      }
+    }
+    slotc++;
+    __syncthreads();
+  }
+  count_proj_points(a, S, a.npl, 1);
+}
+
+// The force pass over the listed nodes (bounds from chi, zee; Ci from ci).
+template <int PM, typename T, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) sweep_force_kernel(SweepArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  Shared &S = *reinterpret_cast<Shared *>(smem);
+  unsigned char *dyn = smem + shared_fixed();
+  double *pcur =
+      reinterpret_cast<double *>(dyn + planes_bytes(a.n) + ring_bytes(a.nsweep, PM) + accw_bytes(a.nsweep, PM));
+  for (int i = threadIdx.x; i < a.n_gproj + PM; i += blockDim.x) pcur[i] = 0.0;  // [n_gproj..]: the empty id
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int q = atomicAdd(a.counter, 1);
+      S.qidx = q;
+      S.node = q < a.n_list ? a.node_list[q] : -1;
+      if (S.node >= 0) {
+        S.gi = S.node % a.np[0];
+        S.gj = (S.node / a.np[0]) % a.np[1];
+        S.gk = S.node / (a.np[0] * a.np[1]);
+      }
+    }
+    __syncthreads();
+    const int node = S.node;
+    if (node < 0) break;
+    double *fs = a.fslots + (size_t)S.qidx * FSLOTS * 4;
+    for (int i = threadIdx.x; i < FSLOTS * 4; i += blockDim.x) fs[i] = (i % 4 == 0) ? -1.0 : 0.0;
+    setup_node(a, S);
+    node_forces<T, PM>(a, S, dyn, pcur, a.chi[node], a.zee[node], a.ci + (size_t)node * (a.npl + 1), fs);
+    __syncthreads();
+  }
+}
+
 // Moments of the quadrature form: mu_j = e_1^T T_j((T_k - chi)/zee) e_1 / h^3
 // on the k-row tridiagonal (one warp, k-vectors in the free window slots).
-__device__ void quadrature_moments(const SweepArgs &a, Shared &S, int k, double chi, double zee, double *mu) {
+static __device__ void quadrature_moments(const SweepArgs &a, Shared &S, int k, double chi, double zee, double *mu) {
   if (threadIdx.x >= 32) return;
   const int lane = threadIdx.x;
   double *v0 = slot<double>(a, 0), *v1 = slot<double>(a, 1), *v2 = slot<double>(a, 2);

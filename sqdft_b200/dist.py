@@ -19,10 +19,10 @@ from .case import Case
 SUM, MIN, MAX = 0, 1, 2
 
 
-def slab(case: Case, rank: int, world: int) -> Case:
-    """The z-slab of the (whole, periodic) grid that `rank` of `world` owns."""
-    if world == 1:
-        return case
+def slab_indices(case: Case, rank: int, world: int):
+    """(z0, planes, kz, ky, kx): the first plane and plane count of `rank`'s
+    z-slab and, per axis, the whole-grid indices of its Veff block with the
+    Rcut halo (periodic wrap), so that veff_slab = veff_grid[kz][:, ky][:, :, kx]."""
     if tuple(case.np_) != tuple(case.n_int):
         raise ValueError("slab decomposition starts from the whole grid")
     nz = case.n_int[2]
@@ -30,11 +30,18 @@ def slab(case: Case, rank: int, world: int) -> Case:
         raise ValueError(f"grid of {nz} planes does not split over {world} ranks")
     sz, z0 = nz // world, rank * (nz // world)
     nl = case.nloc
-    full = case.veff_block
     kz = np.arange(z0 - nl, z0 + sz + nl) % nz
     ky = (np.arange(case.n_int[1] + 2 * nl) - nl) % case.n_int[1]
     kx = (np.arange(case.n_int[0] + 2 * nl) - nl) % case.n_int[0]
-    veff = np.ascontiguousarray(full[np.ix_(kz, ky, kx)])
+    return z0, sz, kz, ky, kx
+
+
+def slab(case: Case, rank: int, world: int) -> Case:
+    """The z-slab of the (whole, periodic) grid that `rank` of `world` owns."""
+    if world == 1:
+        return case
+    z0, sz, kz, ky, kx = slab_indices(case, rank, world)
+    veff = np.ascontiguousarray(case.veff_block[np.ix_(kz, ky, kx)])
     return dataclasses.replace(case, np_=(case.n_int[0], case.n_int[1], sz), pnode_s=(0, 0, z0), veff=veff)
 
 

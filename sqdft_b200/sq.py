@@ -39,7 +39,7 @@ EXPORTS = [
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
     "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check", "sqb_lanczos_moments_nodes",
-    "sqb_set_node_kernel",
+    "sqb_set_node_kernel", "sqb_set_veff_device",
 ]
 
 
@@ -111,6 +111,7 @@ def library() -> C.CDLL:
         lib.sqb_autotune.argtypes = [P, C.c_int, _ip, _dp]
         lib.sqb_set_graph.argtypes = [P, C.c_int]
         lib.sqb_set_node_kernel.argtypes = [P, C.c_int]
+        lib.sqb_set_veff_device.argtypes = [P, C.c_void_p]
         lib.sqb_moments_vjp.argtypes = [P, _dp, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
@@ -234,6 +235,10 @@ class Context:
         if v.size != int(np.prod(self._veff_ext_shape())):
             raise ValueError(f"Veff with halo must have shape {self._veff_ext_shape()}, got {v.shape}")
         _check(self.lib.sqb_set_veff(self.ptr, _d(v)), "sqb_set_veff")
+
+    def set_veff_device(self, ptr: int):
+        """sqb_set_veff_device: Veff with halo from a device pointer (e.g. a torch tensor's data_ptr())."""
+        _check(self.lib.sqb_set_veff_device(self.ptr, C.c_void_p(ptr)), "sqb_set_veff_device")
 
     def set_atoms(self, case: Case):
         types = (SqbSpecies * max(1, len(case.types)))()

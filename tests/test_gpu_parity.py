@@ -339,3 +339,27 @@ def test_sweep_kernel_is_the_default_where_it_applies(golden):
     with _ctx(case) as ctx:
         ctx.lanczos_moments()
         assert ctx.stats()["node_kernel"] == sq.SQB_KERNEL_SWEEP
+
+
+@pytest.mark.parametrize("name", ["tiny", "lihs", "mid"])
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32_mixed"])
+def test_sweep_kernel_forces_match_plane_kernel(golden, name, precision):
+    """ForcesNonLocal (forces.cpp:318-578) on the sweep kernel and on the
+    plane-streaming kernel from the same bounds and coefficients: the same
+    recursion and contraction, summed in another order (FP64 1e-12 Ha/bohr;
+    FP32 recursion vectors 1e-9); in FP64 both match the reference's forces
+    (1e-7 Ha/bohr)."""
+    from sqdft_b200 import sq
+
+    case, ref = golden(name)
+    with _ctx(case, precision) as ctx:
+        out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+        ctx.set_node_kernel(sq.SQB_KERNEL_PLANE)
+        f_plane = ctx.forces_nonlocal(out["chi"], out["zee"], out["Ci"])
+        assert ctx.stats()["node_kernel"] == sq.SQB_KERNEL_PLANE
+        ctx.set_node_kernel(sq.SQB_KERNEL_SWEEP)
+        f_sweep = ctx.forces_nonlocal(out["chi"], out["zee"], out["Ci"])
+        assert ctx.stats()["node_kernel"] == sq.SQB_KERNEL_SWEEP
+    assert np.abs(f_sweep - f_plane).max() <= (1e-12 if precision == 0 else 1e-9)
+    if precision == 0:
+        assert np.abs(f_sweep - ref["fnloc"]).max() <= 1e-7
