@@ -64,6 +64,8 @@ struct Shared {
   double aa[MAXL];
   double bb[MAXL];
   double eig[2], eprev[2];
+  double wdel[2];   // last changes of the extremes (warm start of the next multisection)
+  int warm;         // eig holds the extremes of the previous, one row smaller tridiagonal
   double br[2][2];  // multisection brackets (lambda_min, lambda_max)
   int wres[32];     // per-warp multisection results
   int scan[33];
@@ -329,6 +331,8 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
     load_point(j, 0);
   }
   const double c0 = 3.0 * a.coeff_lap[0];
+  const double rcb = CHEB ? 1.0 / io.cb : 0.0;
+  const double cdh = io.cd / a.h3, ceh = io.ce / a.h3;
 
   for (int z = 0; z < n; z++) {
     T *smz = sm + (z & 1) * P2;
@@ -389,9 +393,11 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
           acc1 += v[j] * hv[j];
           o = (double)ot;
         } else {
+          // sq.cpp:588, 615 divide by zee; the sweep multiplies by 1/zee
+          // (one rounding apart, no FP64 division per point)
           double od;
-          if (io.first) od = (hv[j] - io.ca * v[j]) / io.cb;
-          else od = (2.0 * (hv[j] - io.ca * v[j])) / io.cb - (double)q1[j];
+          if (io.first) od = (hv[j] - io.ca * v[j]) * rcb;
+          else od = (2.0 * (hv[j] - io.ca * v[j])) * rcb - (double)q1[j];
           const T ot = (T)od;
           io.out[g] = ot;
           o = (double)ot;
@@ -399,9 +405,9 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
             acc0 += o * o;
             acc1 += o * v[j];
           }
-          if constexpr (SK == SK_FD) {  // forces.cpp:414-456
-            if (io.first) io.dacc[g] = 0.0 + (g == gc ? 1.0 : 0.0) * io.ce / a.h3 + o * io.cd / a.h3;
-            else io.dacc[g] = dq[j] + o * io.cd / a.h3;
+          if constexpr (SK == SK_FD) {  // forces.cpp:414-456 (Ci / h^3 formed once per sweep)
+            if (io.first) io.dacc[g] = (g == gc ? ceh : 0.0) + o * cdh;
+            else io.dacc[g] = dq[j] + o * cdh;
           }
         }
         if (g == gc) S.center_val = o;
@@ -493,28 +499,29 @@ static __device__ void sweep_sum2(Shared &S, double v0, double v1, int NS) {
 }
 
 // Sturm count: eigenvalues of the leading m x m tridiagonal (d, e) below x,
-// from the sign changes of the characteristic-polynomial sequence, rescaled
-// by exact powers of two to stay in range.
+// from the sign changes of the characteristic-polynomial sequence
+// p_i = (d_i - x) p_i-1 - e_i-1^2 p_i-2, rescaled by exact powers of two every
+// eight rows (a row grows |p| by less than 2^64 here, far inside the range),
+// which leaves every sign and rounding unchanged.  An exact zero counts as
+// positive (a test point on an eigenvalue of a leading submatrix; the
+// multisection's brackets tolerate the one-off count there).
 static __device__ int sturm_count(const double *d, const double *e, int m, double x) {
   double p0 = 1.0, p1 = d[0] - x;
-  int s_prev = 1, cnt = 0;
-  int s1 = p1 > 0.0 ? 1 : (p1 < 0.0 ? -1 : -s_prev);
-  cnt += (s1 != s_prev);
-  s_prev = s1;
+  int cnt = p1 < 0.0;
   for (int i = 1; i < m; i++) {
-    double p2 = (d[i] - x) * p1 - (e[i - 1] * e[i - 1]) * p0;
-    int s2 = p2 > 0.0 ? 1 : (p2 < 0.0 ? -1 : -s_prev);
-    cnt += (s2 != s_prev);
-    s_prev = s2;
+    const double p2 = (d[i] - x) * p1 - (e[i - 1] * e[i - 1]) * p0;
+    cnt += (p2 < 0.0) != (p1 < 0.0);
     p0 = p1;
     p1 = p2;
-    double mx = fmax(fabs(p0), fabs(p1));
-    if (mx > 0x1p+600) {
-      p0 *= 0x1p-600;
-      p1 *= 0x1p-600;
-    } else if (mx < 0x1p-600 && mx > 0.0) {
-      p0 *= 0x1p+600;
-      p1 *= 0x1p+600;
+    if ((i & 7) == 0) {
+      const double mx = fmax(fabs(p0), fabs(p1));
+      if (mx > 0x1p+600) {
+        p0 *= 0x1p-600;
+        p1 *= 0x1p-600;
+      } else if (mx < 0x1p-600 && mx > 0.0) {
+        p0 *= 0x1p+600;
+        p1 *= 0x1p+600;
+      }
     }
   }
   return cnt;
@@ -544,6 +551,19 @@ static __device__ void tridiag_extremes(Shared &S, int m) {
     hi += 1e-14 * span + 1e-300;
     S.br[0][0] = S.br[1][0] = lo;
     S.br[0][1] = S.br[1][1] = hi;
+    if (S.warm) {
+      // Warm start from the previous (one row smaller) tridiagonal's extremes:
+      // by interlacing the new smallest lies at or below the old one and the
+      // new largest at or above it; the other end of each bracket is the old
+      // extreme moved by four times its last change, kept when a Sturm count
+      // confirms that no eigenvalue lies beyond it.
+      const double pad = 16.0 * 2.220446049250313e-16 * span;
+      const double x0 = S.eig[0] - fmax(4.0 * S.wdel[0], 1e-9 * span), x1 = S.eig[1] + fmax(4.0 * S.wdel[1], 1e-9 * span);
+      if (S.eig[0] + pad < hi) S.br[0][1] = S.eig[0] + pad;
+      if (x0 > lo && sturm_count(d, e, m, x0) == 0) S.br[0][0] = x0;
+      if (S.eig[1] - pad > lo) S.br[1][0] = S.eig[1] - pad;
+      if (x1 < hi && sturm_count(d, e, m, x1) == m) S.br[1][1] = x1;
+    }
   }
   __syncthreads();
   auto active = [&](int k) {
@@ -761,6 +781,7 @@ __device__ void lanczos(const SweepArgs &a, Shared &S, unsigned char *dyn, doubl
     S.stop = 0;
     S.count = 0;
     S.eprev[0] = S.eprev[1] = 0.0;
+    S.warm = 0;
   }
   __syncthreads();
   double a_prev = 0.0, s_prev = 1.0, bs_prev = 0.0;
@@ -803,6 +824,9 @@ __device__ void lanczos(const SweepArgs &a, Shared &S, unsigned char *dyn, doubl
         const double dl = fabs(S.eig[0] - S.eprev[0]), dm = fabs(S.eig[1] - S.eprev[1]);
         S.eprev[0] = S.eig[0];
         S.eprev[1] = S.eig[1];
+        S.wdel[0] = S.warm ? dl : 0.0;  // (the first solve's change is against zero)
+        S.wdel[1] = S.warm ? dm : 0.0;
+        S.warm = 1;
         const bool conv = !(dl > a.lanczos_tol || dm > a.lanczos_tol);
         if constexpr (LQ) {
           S.count = m + 1;  // rows of T; the first solve only sets the previous extremes
