@@ -182,6 +182,16 @@ int sqb_set_launch(sqb_ctx *ctx, int ctas_per_sm, int cols_per_thread);
 #define SQB_KERNEL_SWEEP 2
 int sqb_set_node_kernel(sqb_ctx *ctx, int kernel);
 
+/* Test hook of the plane-streaming kernel's bounded waits (its projector
+ * table planes arrive by bulk copies whose completion each plane waits for,
+ * bounded in time).  extra_bytes (a multiple of 16, at most 4096) is added
+ * to every stage's expected byte count, so no stage completes; wait_ms
+ * replaces the 2 s wait limit (0 restores it).  A launch then ends with
+ * SQB_ERR_CUDA after about wait_ms plus a 1 ms grace for the copies already
+ * issued, with no copy in flight, and the context stays usable.  (0, 0)
+ * turns the hook off.  No counterpart in the reference. */
+int sqb_test_stage_wait(sqb_ctx *ctx, unsigned extra_bytes, double wait_ms);
+
 /* CUDA-graph replay of the node-kernel sequence of sqb_lanczos_moments (and
  * so of the SQ step): work-queue and status resets, the persistent Lanczos +
  * Chebyshev launch and the bound min/max, captured on the first call after

@@ -13,7 +13,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
+
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/sqdft_b200.h"
 #include "sqb_internal.cuh"
@@ -92,6 +95,9 @@ struct sqb_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t ev_order = nullptr;  // orders the no-alloc call after the caller's queued work
   sqb_stats stats{};
+  std::string metrics_path;  // SQDFT_B200_METRICS at creation: one JSON line per SQ step / force pass
+  unsigned test_extra_tx = 0;           // sqb_test_stage_wait
+  unsigned long long test_wait_ns = 0;
 };
 
 namespace {
@@ -104,6 +110,33 @@ namespace {
       return SQB_ERR_CUDA;                       \
     }                                            \
   } while (0)
+
+// NVTX range over an entry point (visible in Nsight Systems / Compute; a
+// no-op without a tool attached).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
+// One JSON line per SQ step or force pass into the file named by
+// SQDFT_B200_METRICS (read when the context is created): the phase times,
+// iteration counts and status of the call.
+void write_metrics(const sqb_ctx *c, const char *call, int rc, double lambda_f) {
+  if (c->metrics_path.empty()) return;
+  FILE *f = std::fopen(c->metrics_path.c_str(), "a");
+  if (!f) return;
+  const sqb_stats &s = c->stats;
+  std::fprintf(f,
+               "{\"call\": \"%s\", \"status\": %d, \"precision\": %d, \"node_kernel\": %d, \"nodes\": %d, "
+               "\"window\": %d, \"npl\": %d, \"ms_lanczos_moments\": %.6f, \"ms_fermi\": %.6f, "
+               "\"ms_density\": %.6f, \"ms_defect\": %.6f, \"ms_forces\": %.6f, \"lanczos_iters\": %lld, "
+               "\"max_lanczos_iters\": %d, \"lanczos_maxiter_nodes\": %lld, \"fermi_iters\": %d, "
+               "\"defect_nodes\": %lld, \"matvecs\": %lld, \"kernel_launches\": %d, \"lambda_f\": %.17g}\n",
+               call, rc, c->precision, s.node_kernel, c->nnode, c->n, c->g.npl, s.ms_lanczos_moments, s.ms_fermi,
+               s.ms_density, s.ms_defect, s.ms_forces, s.lanczos_iters, s.max_lanczos_iters, s.lanczos_maxiter_nodes,
+               s.fermi_iters, s.defect_nodes, s.matvecs, s.kernel_launches, lambda_f);
+  std::fclose(f);
+}
 
 template <typename T>
 cudaError_t dalloc(T **p, size_t count) {
@@ -177,6 +210,8 @@ void fill_node_args(sqb_ctx *c, NodeArgs &a) {
   a.lq = c->precision == SQB_FP64_LANCZOS_QUAD;
   a.lanczos_tol = (a.mixed || a.lq) ? std::max(c->g.lanczos_tol, c->mixed_lanczos_tol) : c->g.lanczos_tol;
   a.lz_chk = a.mixed ? c->mixed_lanczos_chk : 0.0;
+  a.test_extra_tx = c->test_extra_tx;
+  a.wait_ns = c->test_wait_ns;
   for (int k = 0; k <= FDN; k++) {
     a.coeff_lap[k] = c->g.coeff_lap[k];
     a.coeff_grad[k] = c->g.coeff_grad[k];
@@ -671,6 +706,7 @@ int sqb_create(const sqb_grid *grid, int device, sqb_ctx **out) {
   CK(cudaMemcpy(c->d_xk, xk.data(), K * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_ctab, ctab.data(), K * K * sizeof(double), cudaMemcpyHostToDevice));
   c->stats.window_points = (long long)c->n * c->n * c->n;
+  if (const char *mp = std::getenv("SQDFT_B200_METRICS")) c->metrics_path = mp;
   *out = c;
   return SQB_OK;
 }
@@ -875,6 +911,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
 }
 
 int sqb_nonlocal_projectors(sqb_ctx *c, double *udvtm_out) {
+  NvtxRange nvtx_range("sqb_nonlocal_projectors");
   if (!c) return SQB_ERR_ARG;
   if (!c->have_atoms || !c->have_tables) return SQB_ERR_STATE;
   cudaSetDevice(c->device);
@@ -963,6 +1000,7 @@ int sqb_hsub_times_vec(sqb_ctx *c, int count, const int *nodes, const double *vi
 
 int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, int *lanczos_iters,
                         double *lambda_min, double *lambda_max) {
+  NvtxRange nvtx_range("sqb_lanczos_moments");
   if (!c) return SQB_ERR_ARG;
   if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
   cudaSetDevice(c->device);
@@ -1125,6 +1163,7 @@ int sqb_ne_constraint(sqb_ctx *c, double lambda_f, double *fval) {
 }
 
 int sqb_fermi_level(sqb_ctx *c, int scf_iter, double lambda_warm, double *lambda_f, int *iters) {
+  NvtxRange nvtx_range("sqb_fermi_level");
   if (!c || !lambda_f) return SQB_ERR_ARG;
   if (!c->have_moments) return SQB_ERR_STATE;
   cudaSetDevice(c->device);
@@ -1144,6 +1183,7 @@ int sqb_fermi_level(sqb_ctx *c, int scf_iter, double lambda_warm, double *lambda
 }
 
 int sqb_density_energy(sqb_ctx *c, double lambda_f, double *rho, double *ci, double *ebs, double *eent) {
+  NvtxRange nvtx_range("sqb_density_energy");
   if (!c) return SQB_ERR_ARG;
   if (!c->have_moments) return SQB_ERR_STATE;
   cudaSetDevice(c->device);
@@ -1178,6 +1218,7 @@ int sqb_density_energy(sqb_ctx *c, double lambda_f, double *rho, double *ci, dou
 // more than half the budget times max rho are redone by the FP64 parity path
 // (the reference's bounds and moments), and the Fermi level is solved again.
 int defect_check(sqb_ctx *c, int scf_iter, double lambda_warm, double *lam) {
+  NvtxRange nvtx_range("sqb_defect_check");
   c->stats.defect_nodes = 0;
   c->stats.ms_defect = 0.0;
   const double tol_eff = std::max(c->g.lanczos_tol, c->mixed_lanczos_tol);
@@ -1252,9 +1293,20 @@ int sqb_set_defect_check(sqb_ctx *c, double budget) {
   return SQB_OK;
 }
 
+static int spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *rho, double *rho_pj, double *ci,
+                               double *chi, double *zee, double *ebs, double *eent);
+
 int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *rho, double *rho_pj, double *ci,
                             double *chi, double *zee, double *ebs, double *eent) {
   if (!c || !lambda_f) return SQB_ERR_ARG;
+  NvtxRange r("sqb_spectral_quadrature");
+  const int rc = spectral_quadrature(c, scf_iter, lambda_f, rho, rho_pj, ci, chi, zee, ebs, eent);
+  write_metrics(c, "spectral_quadrature", rc, *lambda_f);
+  return rc;
+}
+
+static int spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *rho, double *rho_pj, double *ci,
+                               double *chi, double *zee, double *ebs, double *eent) {
   int rc = sqb_lanczos_moments(c, chi, zee, rho_pj, nullptr, nullptr, nullptr);
   if (rc) return rc;
   double lam = 0.0;
@@ -1270,6 +1322,14 @@ int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *
   }
   *lambda_f = lam;
   return sqb_density_energy(c, lam, rho, ci, ebs, eent);
+}
+
+int sqb_test_stage_wait(sqb_ctx *c, unsigned extra_bytes, double wait_ms) {
+  if (!c || !(wait_ms >= 0.0) || wait_ms > 10000.0 || extra_bytes % 16 != 0 || extra_bytes > 4096u)
+    return SQB_ERR_ARG;
+  c->test_extra_tx = extra_bytes;
+  c->test_wait_ns = (unsigned long long)(wait_ms * 1e6);
+  return SQB_OK;
 }
 
 int sqb_set_node_kernel(sqb_ctx *c, int kernel) {
@@ -1436,6 +1496,7 @@ static int ensure_dtab(sqb_ctx *c) {
 }
 
 int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff, double *g_atoms) {
+  NvtxRange nvtx_range("sqb_moments_vjp");
   if (!c || !g_mu || !g_veff) return SQB_ERR_ARG;
   if (!c->have_moments) return SQB_ERR_STATE;
   cudaSetDevice(c->device);
@@ -1504,8 +1565,17 @@ int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff, double *g_at
   return SQB_OK;
 }
 
+static int forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const double *ci, double *forces);
+
 int sqb_forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const double *ci, double *forces) {
   if (!c || !forces) return SQB_ERR_ARG;
+  NvtxRange r("sqb_forces_nonlocal");
+  const int rc = forces_nonlocal(c, chi, zee, ci, forces);
+  write_metrics(c, "forces_nonlocal", rc, 0.0);
+  return rc;
+}
+
+static int forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const double *ci, double *forces) {
   if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
   cudaSetDevice(c->device);
   const size_t N = c->nnode, K = c->g.npl + 1;

@@ -96,6 +96,11 @@ struct NodeArgs {
   size_t vjp_at_stride;  // doubles per CTA
   int *status;
   unsigned long long *proj_points; // algorithmic projector-ball points touched
+  // test hook of the bounded stage waits (sqb_test_stage_wait): bytes added to
+  // every stage's expected transaction count (which then never completes) and
+  // the wait limit in ns (0: the default)
+  unsigned test_extra_tx;
+  unsigned long long wait_ns;
 };
 
 // Layered projector fields of the sweep kernel (sqb_sweep.cuh).  The replica

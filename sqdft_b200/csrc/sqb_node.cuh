@@ -221,13 +221,17 @@ struct RowLanes {
 };
 
 // Announce (one thread) the bytes plane zz's copies will bring into stage st.
-__device__ __forceinline__ void arm_plane(NodeShared &S, int zz, int st, size_t elem) {
-  mbar_arrive_expect_tx(&S.mbar[st], (unsigned)(S.plane_tot[zz] * elem));
+// (not after a stall: the stage's barrier phase never completed, and a second
+// arrival would overrun its count)
+__device__ __forceinline__ void arm_plane(const NodeArgs &a, NodeShared &S, int zz, int st, size_t elem) {
+  if (S.stalled) return;
+  mbar_arrive_expect_tx(&S.mbar[st], (unsigned)(S.plane_tot[zz] * elem) + a.test_extra_tx);
 }
 
 // Issue the bulk copies of plane zz's table planes into stage st, spread
 // over the warps: the k-th box crossing the plane goes to warp k % nw.
 __device__ void issue_plane(const NodeArgs &a, NodeShared &S, unsigned char *dyn, int zz, int st) {
+  if (S.stalled) return;  // no copies after a stall
   const int nw = blockDim.x >> 5;
   const int k = (threadIdx.x & 31) * nw + (threadIdx.x >> 5);
   if (k >= S.ncross[zz]) return;
@@ -245,18 +249,25 @@ __device__ void issue_plane(const NodeArgs &a, NodeShared &S, unsigned char *dyn
 }
 
 // Wait for the copies of a stage (every thread); a wait that runs out of time
-// sets the stall flag and the status bit, after which no further waits are
-// made and the CTA leaves its node loop.
+// (a.wait_ns, default WAIT_NS) gives the copies already issued a further
+// GRACE_NS to land (in-bounds copies take microseconds), then sets the stall
+// flag and the status bit, after which no copies are issued, no stage is armed
+// or waited for, and the CTA leaves its node loop after the current node.
+constexpr unsigned long long GRACE_NS = 1000000ull;
 __device__ __forceinline__ void stage_wait(const NodeArgs &a, NodeShared &S, int st, int &ph) {
   if (!S.stalled) {
     const unsigned parity = (ph >> st) & 1;
+    const unsigned long long limit = a.wait_ns ? a.wait_ns : WAIT_NS;
     bool done = mbar_try_wait(&S.mbar[st], parity);
     if (!done) {
       const unsigned long long t0 = global_ns();
       while (!(done = mbar_try_wait(&S.mbar[st], parity)))
-        if (global_ns() - t0 > WAIT_NS) break;
+        if (global_ns() - t0 > limit) break;
     }
     if (!done) {
+      const unsigned long long t1 = global_ns();
+      while (global_ns() - t1 < GRACE_NS) {
+      }
       S.stalled = 1;
       atomicOr(a.status, ST_WAIT_LIMIT);
     }
@@ -454,7 +465,7 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
   if (STENCIL) {
     for (int i = tid; i < 2 * P2; i += nt) sm_in[i] = T(0);
   }
-  if (staged && tid == 0) arm_plane(S, 0, 0, sizeof(double));
+  if (staged && tid == 0) arm_plane(a, S, 0, 0, sizeof(double));
   __syncthreads();
   int ph = S.ph;
   if (staged) issue_plane(a, S, dyn, 0, 0);
@@ -564,7 +575,7 @@ __device__ void pass(const NodeArgs &a, NodeShared &S, unsigned char *dyn, const
     }
     const int st_next = st == NSTAGE - 1 ? 0 : st + 1, st_prev = st == 0 ? NSTAGE - 1 : st - 1;
     if (staged && z < n) stage_wait(a, S, st, ph);
-    if (staged && tid == 0 && z + 1 < n) arm_plane(S, z + 1, st_next, sizeof(double));
+    if (staged && tid == 0 && z + 1 < n) arm_plane(a, S, z + 1, st_next, sizeof(double));
     __syncthreads();
     if (DOTS && z >= 1 && S.n_ent > 0)
       dot_phase<T>(S, sm_out + ((z - 1) & 1) * n2, z - 1, n, tab, off_tab + (z - 1) * MAXE,
@@ -733,7 +744,7 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
   if (STENCIL) {
     for (int i = tid; i < 2 * RPLANE; i += nt) sm_in[i] = T(0);
   }
-  if (staged && tid == 0) arm_plane(S, 0, 0, sizeof(double));
+  if (staged && tid == 0) arm_plane(a, S, 0, 0, sizeof(double));
   __syncthreads();
   int ph = S.ph;
   if (staged) issue_plane(a, S, dyn, 0, 0);
@@ -829,7 +840,7 @@ __device__ void pass_rows(const NodeArgs &a, NodeShared &S, unsigned char *dyn, 
     }
     const int st_next = st == NSTAGE - 1 ? 0 : st + 1, st_prev = st == 0 ? NSTAGE - 1 : st - 1;
     if (staged && z < n) stage_wait(a, S, st, ph);
-    if (staged && tid == 0 && z + 1 < n) arm_plane(S, z + 1, st_next, sizeof(double));
+    if (staged && tid == 0 && z + 1 < n) arm_plane(a, S, z + 1, st_next, sizeof(double));
     __syncthreads();
     if (DOTS && z >= 1 && S.n_ent > 0)
       dot_phase<T>(S, sm_out + ((z - 1) & 1) * OPLANE, z - 1, 32, tab, off_tab + (z - 1) * MAXE,

@@ -39,7 +39,7 @@ EXPORTS = [
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
     "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check", "sqb_lanczos_moments_nodes",
-    "sqb_set_node_kernel", "sqb_set_veff_device",
+    "sqb_set_node_kernel", "sqb_set_veff_device", "sqb_test_stage_wait",
 ]
 
 
@@ -112,6 +112,7 @@ def library() -> C.CDLL:
         lib.sqb_set_graph.argtypes = [P, C.c_int]
         lib.sqb_set_node_kernel.argtypes = [P, C.c_int]
         lib.sqb_set_veff_device.argtypes = [P, C.c_void_p]
+        lib.sqb_test_stage_wait.argtypes = [P, C.c_uint, C.c_double]
         lib.sqb_moments_vjp.argtypes = [P, _dp, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
@@ -235,6 +236,10 @@ class Context:
         if v.size != int(np.prod(self._veff_ext_shape())):
             raise ValueError(f"Veff with halo must have shape {self._veff_ext_shape()}, got {v.shape}")
         _check(self.lib.sqb_set_veff(self.ptr, _d(v)), "sqb_set_veff")
+
+    def test_stage_wait(self, extra_bytes: int = 0, wait_ms: float = 0.0):
+        """sqb_test_stage_wait (test hook of the plane-streaming kernel's bounded waits)."""
+        _check(self.lib.sqb_test_stage_wait(self.ptr, int(extra_bytes), float(wait_ms)), "sqb_test_stage_wait")
 
     def set_veff_device(self, ptr: int):
         """sqb_set_veff_device: Veff with halo from a device pointer (e.g. a torch tensor's data_ptr())."""

@@ -80,3 +80,49 @@ def test_lanczos_cap_is_a_counted_warning(golden):
     assert np.all(ref["lanczos_iters"][nodes] == 500)
     assert np.abs(m["chi"] - ref["chi"][nodes]).max() <= 1e-9
     assert np.abs(m["zee"] - ref["zee"][nodes]).max() <= 1e-9
+
+
+def test_metrics_record_per_call(golden, tmp_path, monkeypatch):
+    """SQDFT_B200_METRICS names a file that receives one JSON line per SQ step
+    and per force pass: phase times, iteration counts, status."""
+    import json
+
+    from sqdft_b200 import sq
+
+    case, _ = golden("tiny")
+    path = tmp_path / "metrics.jsonl"
+    monkeypatch.setenv("SQDFT_B200_METRICS", str(path))
+    with sq.Context(case, device=0) as ctx:
+        ctx.set_projectors(case.udvtm)
+        out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+        ctx.forces_nonlocal()
+        st = ctx.stats()
+    lines = [json.loads(s) for s in path.read_text().splitlines()]
+    assert [r["call"] for r in lines] == ["spectral_quadrature", "forces_nonlocal"]
+    sq_rec = lines[0]
+    assert sq_rec["status"] == 0 and sq_rec["nodes"] == case.n_nodes and sq_rec["npl"] == case.npl
+    assert sq_rec["lambda_f"] == out["lambda_f"]
+    assert sq_rec["lanczos_iters"] > 0 and sq_rec["ms_lanczos_moments"] > 0.0
+    assert abs(lines[1]["ms_forces"] - st["ms_forces"]) <= 1e-5
+
+
+def test_bounded_stage_wait_runs_out_cleanly(golden):
+    """The plane-streaming kernel's waits for its bulk-copied table planes are
+    bounded: with the test hook every stage expects 16 bytes more than its
+    copies bring, each wait gives up after 1 ms (plus the 1 ms grace for the
+    copies already issued), the call returns SQB_ERR_CUDA, and the context
+    runs the next step normally with the hook off."""
+    from sqdft_b200 import sq
+
+    case, ref = golden("tiny")
+    with sq.Context(case, device=0) as ctx:
+        ctx.set_projectors(case.udvtm)
+        ctx.set_node_kernel(sq.SQB_KERNEL_PLANE)
+        ctx.test_stage_wait(16, 1.0)
+        with pytest.raises(sq.SQBError) as err:
+            ctx.lanczos_moments()
+        assert err.value.code == 2  # SQB_ERR_CUDA
+        ctx.test_stage_wait(0, 0.0)
+        m = ctx.lanczos_moments()
+    assert np.abs(m["chi"] - ref["chi"]).max() <= 1e-10
+    assert np.abs(m["zee"] - ref["zee"]).max() <= 1e-10
