@@ -299,6 +299,23 @@ int sqb_moments_at(sqb_ctx *ctx, const double *chi, const double *zee, double *r
  * reference. */
 int sqb_moments_vjp(sqb_ctx *ctx, const double *g_mu, double *g_veff, double *g_atoms);
 
+/* Forward and backward of a density loss L = sum_p w[p] rho[p] (the density
+ * of the last sqb_density_energy, w per node of the block, reduced over
+ * ranks), the bounds held fixed.  sqb_density_loss gives L.
+ * sqb_density_loss_vjp gives grad_l * dL/dVeff on the Veff block with its halo
+ * (layout of sqb_set_veff) and, when g_atoms is not NULL, grad_l * dL/dR
+ * [n_atm][3]: one moment adjoint (sqb_moments_vjp) with weights
+ * 2 grad_l (w_p - kappa h^3) sign(rho_p) c_j(p), where with
+ * fixed_electrons = 0 the Fermi level is held (kappa = 0) and otherwise the
+ * electron count (the SCF's constraint): kappa = (dL/dlambda) / (dN_e/dlambda),
+ * the lambda-derivatives from the Chebyshev coefficients of beta f (1 - f) on
+ * each node's interval.  Needs a prior sqb_density_energy (its Fermi level and
+ * coefficients).  This pair is the forward/backward of a
+ * torch.autograd.Function.  No counterpart in the reference. */
+int sqb_density_loss(sqb_ctx *ctx, const double *w, double *loss);
+int sqb_density_loss_vjp(sqb_ctx *ctx, const double *w, int fixed_electrons, double grad_l, double *g_veff,
+                         double *g_atoms);
+
 /* Size of the fixed device scratch array used by sqb_lanczos_moments_noalloc
  * (held on every GPU that loads the library, until the process exits). */
 #define SQB_NOALLOC_SCRATCH_BYTES (64u << 20)

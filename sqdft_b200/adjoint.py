@@ -81,12 +81,19 @@ class DensityLoss:
         if self.fixed_electrons:
             self.lam, _ = ctx.fermi_level(self.scf_iter, self.lam)
         dens = ctx.density_energy(self.lam)
-        rho = dens["rho"].reshape(-1)
-        w = np.asarray(w, np.float64).reshape(-1)
-        self.saved = (mu, dens["Ci"], rho, w)
-        return float(np.dot(w, rho))
+        w = np.ascontiguousarray(w, np.float64).reshape(-1)
+        self.saved = (mu, dens["Ci"], dens["rho"].reshape(-1), w)
+        return ctx.density_loss(w)  # sqb_density_loss
 
     def backward(self, grad_l: float = 1.0) -> np.ndarray:
+        """grad_l dL/dVeff by sqb_density_loss_vjp (the lambda response and the
+        moment weights on the device, then the moment adjoint)."""
+        w = self.saved[3]
+        return self.ctx.density_loss_vjp(w, fixed_electrons=self.fixed_electrons, grad_l=grad_l)
+
+    def backward_host(self, grad_l: float = 1.0) -> np.ndarray:
+        """The same gradient with the moment weights formed on the host (the
+        check of sqb_density_loss_vjp's weights)."""
         mu, ci, rho, w = self.saved
         sign = np.sign(rho)
         weight = w * sign

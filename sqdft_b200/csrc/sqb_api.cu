@@ -87,6 +87,9 @@ struct sqb_ctx {
   double *d_xk = nullptr, *d_ctab = nullptr, *d_partial = nullptr, *d_result = nullptr;
   double *d_rho = nullptr, *d_ci = nullptr;
   double *d_sens = nullptr;  // per-node density sensitivity of the defect check
+  double *d_loss = nullptr;  // density-loss adjoint: weights and signs [2][N]
+  int loss_n = 0;
+  double lambda_last = 0.0;  // Fermi level of the last sqb_density_energy
   bool have_ci = false;
   double *d_fslots = nullptr, *d_f = nullptr;
   double *d_tmp = nullptr;
@@ -720,7 +723,7 @@ int sqb_destroy(sqb_ctx *c) {
                   c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
                   c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
-                  c->d_f, c->d_tmp, c->d_sens};
+                  c->d_f, c->d_tmp, c->d_sens, c->d_loss};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   drop_graph(c);
@@ -1199,6 +1202,7 @@ int sqb_density_energy(sqb_ctx *c, double lambda_f, double *rho, double *ci, dou
   CK(cudaStreamSynchronize(c->stream));
   c->stats.ms_density = elapsed(c);
   c->have_ci = true;
+  c->lambda_last = lambda_f;
   if (st & 2) return SQB_ERR_NONFINITE;
   int rc = reduce(c, r, 2, SQB_SUM);
   if (rc) return rc;
@@ -1495,11 +1499,13 @@ static int ensure_dtab(sqb_ctx *c) {
   return SQB_OK;
 }
 
-int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff, double *g_atoms) {
-  NvtxRange nvtx_range("sqb_moments_vjp");
-  if (!c || !g_mu || !g_veff) return SQB_ERR_ARG;
-  if (!c->have_moments) return SQB_ERR_STATE;
-  cudaSetDevice(c->device);
+}  // extern "C"
+
+// Moment adjoint on the plane-streaming kernel (node_vjp): buffers, then the
+// weights dL/dmu [N][npl+1] filled by `fill` into the device array it is
+// given (a copy from the host, or a kernel), then the launch.
+template <typename Fill>
+static int moments_vjp(sqb_ctx *c, Fill fill, double *g_veff, double *g_atoms) {
   const size_t N = c->nnode, K = c->g.npl + 1;
   const size_t nw = (size_t)c->n * c->n * c->n;
   const size_t ext = (size_t)c->ex * c->ey * c->ez;
@@ -1532,7 +1538,8 @@ int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff, double *g_at
     d_gat = c->d_vjp_at + per_at * grid;
     CK(cudaMemsetAsync(d_gat, 0, (size_t)3 * std::max(c->n_atm, 1) * sizeof(double), c->stream));
   }
-  CK(cudaMemcpyAsync(d_g, g_mu, N * K * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = fill(d_g);
+  if (rc) return rc;
   CK(cudaMemsetAsync(d_out, 0, ext * sizeof(double), c->stream));
   NodeArgs a;
   fill_node_args(c, a);
@@ -1551,7 +1558,7 @@ int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff, double *g_at
     a.vjp_at_stride = per_at;
   }
   CK(cudaEventRecord(c->ev0, c->stream));
-  int rc = run_nodes(c, a, c->d_nodes, c->nnode);
+  rc = run_nodes(c, a, c->d_nodes, c->nnode);
   if (rc) return rc;
   CK(cudaEventRecord(c->ev1, c->stream));
   rc = read_status(c);
@@ -1565,6 +1572,72 @@ int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff, double *g_at
   return SQB_OK;
 }
 
+extern "C" {
+
+int sqb_moments_vjp(sqb_ctx *c, const double *g_mu, double *g_veff, double *g_atoms) {
+  NvtxRange nvtx_range("sqb_moments_vjp");
+  if (!c || !g_mu || !g_veff) return SQB_ERR_ARG;
+  if (!c->have_moments) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  const size_t NK = (size_t)c->nnode * (c->g.npl + 1);
+  return moments_vjp(
+      c,
+      [&](double *d_g) -> int {
+        CK(cudaMemcpyAsync(d_g, g_mu, NK * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        return SQB_OK;
+      },
+      g_veff, g_atoms);
+}
+
+int sqb_density_loss(sqb_ctx *c, const double *w, double *loss) {
+  if (!c || !w || !loss) return SQB_ERR_ARG;
+  if (!c->have_ci) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  std::vector<double> rho(c->nnode);
+  CK(cudaMemcpy(rho.data(), c->d_rho, rho.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  double l = 0.0;
+  for (int p = 0; p < c->nnode; p++) l += w[p] * rho[p];
+  const int rc = reduce(c, &l, 1, SQB_SUM);
+  if (rc) return rc;
+  *loss = l;
+  return SQB_OK;
+}
+
+int sqb_density_loss_vjp(sqb_ctx *c, const double *w, int fixed_electrons, double grad_l, double *g_veff,
+                         double *g_atoms) {
+  NvtxRange nvtx_range("sqb_density_loss_vjp");
+  if (!c || !w || !g_veff || !std::isfinite(grad_l)) return SQB_ERR_ARG;
+  if (!c->have_moments || !c->have_ci) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  const int N = c->nnode, K = c->g.npl + 1;
+  if (c->loss_n < N) {
+    CK(dalloc(&c->d_loss, (size_t)2 * std::max(N, 1)));
+    c->loss_n = N;
+  }
+  double *d_w = c->d_loss, *d_sgn = c->d_loss + N;
+  CK(cudaMemcpyAsync(d_w, w, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_loss_lambda(fermi_args(c), c->lambda_last, d_w, fixed_electrons ? 1 : 0, d_sgn, c->stream));
+  double sums[2];
+  CK(cudaMemcpyAsync(sums, c->d_result, sizeof(sums), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int rc = reduce(c, sums, 2, SQB_SUM);
+  if (rc) return rc;
+  // a fixed electron count N_e = h^3 sum_p rho_p moves the Fermi level with
+  // Veff: dL/dVeff = dL/dVeff|_lambda - kappa dN_e/dVeff|_lambda,
+  // kappa = (dL/dlambda) / (dN_e/dlambda), one adjoint with weights w - kappa h^3
+  double off = 0.0;
+  if (fixed_electrons) {
+    if (!(sums[1] != 0.0) || !std::isfinite(sums[0] / sums[1])) return SQB_ERR_NONFINITE;
+    off = sums[0] / sums[1];  // kappa h^3
+  }
+  return moments_vjp(
+      c,
+      [&](double *d_g) -> int {
+        CK(launch_loss_gmu(N, K, c->d_ci, d_w, d_sgn, 2.0 * grad_l, off, d_g, c->stream));
+        return SQB_OK;
+      },
+      g_veff, g_atoms);
+}
 static int forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const double *ci, double *forces);
 
 int sqb_forces_nonlocal(sqb_ctx *c, const double *chi, const double *zee, const double *ci, double *forces) {

@@ -163,6 +163,65 @@ __global__ void __launch_bounds__(256) bound_sens_kernel(FermiArgs a, double lam
   }
 }
 
+// Adjoint of a density loss L = sum_p w_p rho_p, rho_p = |2 c(lambda) . mu_p|
+// (sq.cpp:743-797), the bounds held fixed: per node the sign s_p of 2 c . mu_p
+// into sgn and, with a fixed electron count, the density's derivative with
+// respect to the Fermi level, drho_p/dlambda = 2 s_p dc/dlambda . mu_p, where
+// dc/dlambda are the Chebyshev coefficients (ChebyshevCoeff, sq.cpp:1230-1259)
+// of d f/d lambda = beta f (1 - f) on the node's interval; block partials of
+// sum_p w_p drho_p/dlambda and sum_p drho_p/dlambda.  One warp per node.
+__global__ void __launch_bounds__(FTHREADS) loss_lambda_kernel(FermiArgs a, double lambda, const double *w,
+                                                               int fixed, double *sgn, int fits) {
+  extern __shared__ __align__(16) double fsm[];
+  __shared__ double red[FW][2];
+  const int K = a.npl + 1;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  double *dk = fsm + (fits ? K * K : 0) + (size_t)wp * K;
+  const double *ctab = stage_table(a.ctab, fsm, K, fits);
+  double pw = 0.0, pn = 0.0;
+  for (int node = blockIdx.x * FW + wp; node < a.n_nodes; node += gridDim.x * FW) {
+    const double *mu = a.rho_pj + (size_t)node * K;
+    const double *ci = a.ci + (size_t)node * K;
+    double r = 0.0;
+    for (int j = lane; j < K; j += 32) r = r + 2 * mu[j] * ci[j];
+    r = wsum(r);
+    const double sg = (double)((r > 0.0) - (r < 0.0));
+    if (fixed) {
+      const double zee = a.zee[node], chi = a.chi[node];
+      const double lambda_fp = (lambda - chi) / zee, bet = a.bet0 * zee;
+      for (int k = lane; k < K; k += 32) {
+        const double f = 1 / (1 + exp(bet * (a.xk[k] - lambda_fp)));
+        dk[k] = a.bet0 * f * (1 - f);
+      }
+      __syncwarp();
+      double d = 0.0;
+      for (int j = lane; j < K; j += 32) d = d + 2 * mu[j] * cheb_coeff(dk, ctab, K, j);
+      d = wsum(d) * sg;
+      if (lane == 0) {
+        pw += w[node] * d;
+        pn += d;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) sgn[node] = sg;
+  }
+  bsum2(pw, pn, red);
+  if (threadIdx.x == 0) {
+    a.partial[2 * blockIdx.x] = pw;
+    a.partial[2 * blockIdx.x + 1] = pn;
+  }
+}
+
+// Moment weights of the loss: g[p][j] = scale (w_p - off) s_p Ci[p][j].
+__global__ void loss_gmu_kernel(int n, int K, const double *ci, const double *w, const double *sgn, double scale,
+                                double off, double *g) {
+  const long long total = (long long)n * K;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int p = (int)(i / K);
+    g[i] = scale * (w[p] - off) * sgn[p] * ci[i];
+  }
+}
+
 __global__ void sum_partials(const double *partial, int nblocks, int width, double *out) {
   __shared__ double red[32][2];
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -448,6 +507,24 @@ cudaError_t launch_density_energy(const FermiArgs &a, double lambda, cudaStream_
   const int nb = fermi_blocks(a.n_nodes);
   density_kernel<<<nb, FTHREADS, smem, s>>>(a, lambda, fits ? 1 : 0);
   sum_partials<<<1, 1024, 0, s>>>(a.partial, nb, 2, a.result);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loss_lambda(const FermiArgs &a, double lambda, const double *w, int fixed, double *sgn,
+                               cudaStream_t s) {
+  bool fits;
+  const size_t smem = fermi_smem(a.npl + 1, 1, fits);
+  cudaFuncSetAttribute(loss_lambda_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int nb = fermi_blocks(a.n_nodes);
+  loss_lambda_kernel<<<nb, FTHREADS, smem, s>>>(a, lambda, w, fixed, sgn, fits ? 1 : 0);
+  sum_partials<<<1, 1024, 0, s>>>(a.partial, nb, 2, a.result);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loss_gmu(int n, int K, const double *ci, const double *w, const double *sgn, double scale,
+                            double off, double *g, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  loss_gmu_kernel<<<592, 256, 0, s>>>(n, K, ci, w, sgn, scale, off, g);
   return cudaGetLastError();
 }
 

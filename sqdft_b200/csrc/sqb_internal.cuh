@@ -208,6 +208,12 @@ struct FermiArgs {
 cudaError_t launch_ne_constraint(const FermiArgs &a, double lambda, int with_derivative, cudaStream_t s);
 cudaError_t launch_density_energy(const FermiArgs &a, double lambda, cudaStream_t s);
 int fermi_blocks(int n_nodes);
+// Density-loss adjoint (sqb_density_loss_vjp): signs of the nodes' densities
+// and the Fermi-level response sums into result[0..1]; then the moment weights.
+cudaError_t launch_loss_lambda(const FermiArgs &a, double lambda, const double *w, int fixed, double *sgn,
+                               cudaStream_t s);
+cudaError_t launch_loss_gmu(int n, int K, const double *ci, const double *w, const double *sgn, double scale,
+                            double off, double *g, cudaStream_t s);
 cudaError_t launch_bound_sens(const FermiArgs &a, double lambda, double delta, double *sens, double *rho0,
                               cudaStream_t s);
 

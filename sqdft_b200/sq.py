@@ -39,7 +39,8 @@ EXPORTS = [
     "sqb_spectral_quadrature", "sqb_forces_nonlocal", "sqb_get_stats", "sqb_status_string", "sqb_version",
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
     "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check", "sqb_lanczos_moments_nodes",
-    "sqb_set_node_kernel", "sqb_set_veff_device", "sqb_test_stage_wait",
+    "sqb_set_node_kernel", "sqb_set_veff_device", "sqb_test_stage_wait", "sqb_density_loss",
+    "sqb_density_loss_vjp",
 ]
 
 
@@ -113,6 +114,8 @@ def library() -> C.CDLL:
         lib.sqb_set_node_kernel.argtypes = [P, C.c_int]
         lib.sqb_set_veff_device.argtypes = [P, C.c_void_p]
         lib.sqb_test_stage_wait.argtypes = [P, C.c_uint, C.c_double]
+        lib.sqb_density_loss.argtypes = [P, _dp, _dp]
+        lib.sqb_density_loss_vjp.argtypes = [P, _dp, C.c_int, C.c_double, _dp, _dp]
         lib.sqb_moments_vjp.argtypes = [P, _dp, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
@@ -236,6 +239,23 @@ class Context:
         if v.size != int(np.prod(self._veff_ext_shape())):
             raise ValueError(f"Veff with halo must have shape {self._veff_ext_shape()}, got {v.shape}")
         _check(self.lib.sqb_set_veff(self.ptr, _d(v)), "sqb_set_veff")
+
+    def density_loss(self, w: np.ndarray) -> float:
+        """sqb_density_loss: sum_p w_p rho_p of the last density."""
+        w = np.ascontiguousarray(w, np.float64).reshape(-1)
+        out = C.c_double()
+        _check(self.lib.sqb_density_loss(self.ptr, _d(w), C.byref(out)), "sqb_density_loss")
+        return out.value
+
+    def density_loss_vjp(self, w: np.ndarray, fixed_electrons: bool = True, grad_l: float = 1.0,
+                         atoms: bool = False):
+        """sqb_density_loss_vjp: grad_l dL/dVeff (Veff block with halo), and dL/dR with atoms=True."""
+        w = np.ascontiguousarray(w, np.float64).reshape(-1)
+        g = np.zeros(self._veff_ext_shape())
+        ga = np.zeros((self.case.n_atm, 3)) if atoms else None
+        _check(self.lib.sqb_density_loss_vjp(self.ptr, _d(w), int(bool(fixed_electrons)), float(grad_l), _d(g),
+                                             _d(ga)), "sqb_density_loss_vjp")
+        return (g, ga) if atoms else g
 
     def test_stage_wait(self, extra_bytes: int = 0, wait_ms: float = 0.0):
         """sqb_test_stage_wait (test hook of the plane-streaming kernel's bounded waits)."""

@@ -310,3 +310,62 @@ def test_atom_gradient_converges_to_reference_nonlocal_forces():
     assert abs(f20 - f14) <= 0.05 * f20  # the same physical force on both grids
     assert gap20 <= 0.08 * f20
     assert gap20 <= 0.45 * gap14
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64_bounds", "fp32_mixed_bounds"])
+def test_density_loss_adjoint_configuration(precision):
+    """The adjoint configuration c4 (32 Al atoms, 32^3 grid, 27^3 windows,
+    npl 64, kT 5 eV): L = sum_x w(x) rho(x) with seeded uniform w in [0, 1] at
+    a fixed electron count, the bounds of the FP64 or the FP32-mixed Lanczos
+    held fixed (the FP32-mixed form's moments and adjoint recursion are FP64,
+    so its adjoint is this one at its own bounds).  The C++ pair
+    (sqb_density_loss, sqb_density_loss_vjp: Fermi-level response and moment
+    weights on the device, checkpoints every 8 recursion steps) gives the
+    gradient the host-formed weights give to 1e-12; it matches central
+    differences (step 1e-4) of the whole forward along random Veff directions
+    to 1e-6 relative, and the atom gradient matches central differences of
+    moved atoms (tables recomputed on the GPU) to 1e-6 of max |dL/dR|."""
+    import dataclasses
+
+    from sqdft_b200 import sq
+    from sqdft_b200.adjoint import DensityLoss
+    from sqdft_b200.cases import load
+
+    case = dataclasses.replace(load("c4"), fermi_tol=1e-14)
+    rng = np.random.default_rng(44)
+    h3 = case.delta ** 3
+    with sq.Context(case, device=0, precision=precision) as ctx:
+        ctx.set_mixed_lanczos(0.0)
+        ctx.nonlocal_projectors()
+        out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+        m = ctx.lanczos_moments()
+        runner = DensityLoss(ctx, m["chi"], m["zee"], case.bet, h3, fixed_electrons=True, scf_iter=2,
+                             lambda_warm=out["lambda_f"])
+        w = rng.uniform(0.0, 1.0, size=case.n_nodes)
+        runner.forward(case.veff, w)
+        g_ext = runner.backward(1.0)
+        g_host = runner.backward_host(1.0)
+        assert np.abs(g_ext - g_host).max() <= 1e-12 * np.abs(g_ext).max()
+        g_v, g_at = ctx.density_loss_vjp(w, fixed_electrons=True, grad_l=1.0, atoms=True)
+        assert np.abs(g_v - g_ext).max() <= 1e-12 * np.abs(g_ext).max()
+        grad = _fold(case, g_ext)
+        for trial in range(2):
+            d = rng.uniform(-1.0, 1.0, size=int(np.prod(case.n_int)))
+            fd = _directional(case, runner, w, d)
+            an = float(np.dot(grad, d))
+            assert abs(fd - an) <= 1e-6 * abs(an), (trial, fd, an)
+        scale = np.abs(g_at).max()
+        assert scale > 0
+        eps = 1e-4
+        for atom, al in ((0, 0), (case.n_atm // 2, 2)):
+            vals = []
+            for s in (+1, -1):
+                xyz = case.rep_xyz.copy()
+                xyz[case.rep_atom == atom, al] += s * eps
+                ctx.set_atoms(dataclasses.replace(case, rep_xyz=xyz))
+                ctx.nonlocal_projectors()
+                vals.append(runner.forward(case.veff, w))
+            ctx.set_atoms(case)
+            ctx.nonlocal_projectors()
+            fd = (vals[0] - vals[1]) / (2 * eps)
+            assert abs(fd - g_at[atom, al]) <= 1e-6 * scale, (atom, al, fd, g_at[atom, al], scale)
