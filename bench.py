@@ -146,6 +146,7 @@ def run_sample(args):
     nodes = (np.arange(k, dtype=np.int64) * case.n_nodes // k).astype(np.int32)
     with sq.Context(case, device=0, precision=prec) as ctx:
         ctx.set_mixed_lanczos(args.mixed_lanczos_tol)
+        ctx.set_sweep_rows(args.sweep_rows)
         ctx.nonlocal_projectors()
         for _ in range(args.warmup):
             ctx.lanczos_moments_nodes(nodes)
@@ -162,6 +163,36 @@ def run_sample(args):
                       "lanczos_iters_per_node": st["lanczos_iters"] / k, "algorithmic_bytes": abytes,
                       "achieved_gbs": abytes / kern / 1e9, "peak": peak, "peak_kind": peak_kind,
                       "frac": abytes / kern / 1e9 / peak}), flush=True)
+
+
+def run_forces(args):
+    """ForcesNonLocal (forces.cpp:318-578) alone on a configuration after one
+    SQ step of the given precision: W untimed and S timed force passes; one
+    JSON line with the kernel time.  For profiling the force kernel."""
+    import torch
+
+    from sqdft_b200 import sq
+    from sqdft_b200.cases import load as load_named
+
+    torch.cuda.set_device(0)
+    case = load_named(args.config)
+    prec = {"fp64": sq.SQB_FP64, "mixed": sq.SQB_FP32_MIXED, "all": sq.SQB_FP64}[args.precision]
+    with sq.Context(case, device=0, precision=prec) as ctx:
+        ctx.set_sweep_rows(args.sweep_rows)
+        ctx.nonlocal_projectors()
+        ctx.spectral_quadrature(case.scf_iter, case.lambda_f, outputs=False)
+        for _ in range(args.warmup):
+            ctx.forces_nonlocal()
+        ms = []
+        for _ in range(args.steps):
+            f = ctx.forces_nonlocal()
+            st = ctx.stats()
+            ms.append(st["ms_forces"])
+    kern = float(np.mean(ms)) * 1e-3
+    print(json.dumps({"mode": "forces", "config": args.config, "precision": args.precision, "nodes": case.n_nodes,
+                      "kernel_ms": kern * 1e3, "nodes_per_s": case.n_nodes / kern,
+                      "kernel": "sweep_force_kernel" if st["node_kernel"] == sq.SQB_KERNEL_SWEEP else "node_kernel",
+                      "max_abs_force": float(np.abs(f).max())}), flush=True)
 
 
 def run_ours(args):
@@ -186,6 +217,7 @@ def run_ours(args):
 
     ctx = sq.Context(my, device=local, precision=first, allreduce=allreduce_fn(dist, "cuda") if ws > 1 else None)
     ctx.set_mixed_lanczos(args.mixed_lanczos_tol)
+    ctx.set_sweep_rows(args.sweep_rows)
     ctx.nonlocal_projectors()
     n = my.n_nodes
     K1 = my.npl + 1
@@ -507,9 +539,15 @@ def main():
     ap.add_argument("--no-forces", action="store_true", help="skip the nonlocal-force timing")
     ap.add_argument("--sample-nodes", type=int, default=0,
                     help="time the node kernel alone on this many nodes (needs --precision fp64|mixed|lq)")
+    ap.add_argument("--sweep-rows", type=int, default=0, choices=[0, 2, 3],
+                    help="window rows per sweep-kernel thread (0: the library's choice)")
+    ap.add_argument("--forces-only", action="store_true",
+                    help="one SQ step, then time ForcesNonLocal alone (needs --precision fp64|mixed)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.forces_only:
+        run_forces(args)
     else:
         run_ours(args)
 

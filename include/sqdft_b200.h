@@ -181,6 +181,17 @@ int sqb_set_launch(sqb_ctx *ctx, int ctas_per_sm, int cols_per_thread);
 #define SQB_KERNEL_PLANE 1
 #define SQB_KERNEL_SWEEP 2
 int sqb_set_node_kernel(sqb_ctx *ctx, int kernel);
+/* Window rows per thread of the sweep kernel: 2 (one column and two rows per
+ * thread, the default), 3 (fewer threads, more registers each; windows up to
+ * 33 wide), or 0 for the default.  Results agree to rounding (the block
+ * reductions sum in another order). */
+int sqb_set_sweep_rows(sqb_ctx *ctx, int rows);
+/* Times the SQ node work on the sweep kernel with two and with three rows
+ * per thread on `sample` evenly spaced nodes (0: two per SM), keeps the
+ * faster for the context; *rows the choice, ms[2] the times (-1 where a
+ * variant does not apply).  SQB_ERR_UNSUPPORTED when the sweep kernel does
+ * not cover the context. */
+int sqb_autotune_sweep(sqb_ctx *ctx, int sample, int *rows, double *ms);
 
 /* Test hook of the plane-streaming kernel's bounded waits (its projector
  * table planes arrive by bulk copies whose completion each plane waits for,

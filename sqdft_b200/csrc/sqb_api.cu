@@ -67,6 +67,7 @@ struct sqb_ctx {
   // Sweep kernel (sqb_sweep.cuh) and its layered projector fields, built on
   // first use after the projector tables are set.
   int node_kernel = SQB_KERNEL_AUTO;
+  int sweep_ry = 0;  // window rows per sweep-kernel thread (0: automatic)
   int lay_state = 0;  // 0 not built, 1 built and usable, -1 the sweep kernel does not cover this context
   int n_gproj = 0, lay_pmax = 1, n_lrep = 0;
   unsigned long long *d_lay_id = nullptr;
@@ -325,7 +326,8 @@ int ensure_layers(sqb_ctx *c) {
   const long long evol_all = (long long)c->ex * c->ey * c->ez;
   const bool usable = (int)layers.size() <= LAYERS && pmax <= LAY_PMAX && ngp + pm < 65535 &&
                       evol_all * LAYERS * LAY_PMAX < (1LL << 31) &&
-                      sweep_threads(c->n) <= 1024 && sweep_smem(c->n, pm, ngp) <= (size_t)optin && c->n_typ < 256;
+                      sweep_rows_supported(c->n, 2) && sweep_smem(c->n, pm, ngp, 2) <= (size_t)optin &&
+                      c->n_typ < 256;
   if (!usable) return SQB_OK;
   const long long evol = (long long)c->ex * c->ey * c->ez;
   c->n_gproj = ngp;
@@ -387,6 +389,21 @@ int ensure_sweep_scratch(sqb_ctx *c, int grid, size_t *stride) {
   return SQB_OK;
 }
 
+// Window rows per sweep-kernel thread: the requested count where the kernel
+// covers it (sqb_set_sweep_rows, sqb_autotune_sweep), else 2.  (Three rows
+// give fewer threads more registers; measured on the B200 they were slower
+// also where the fields carry three projectors per slot: c3 FP64 199 against
+// 167 ms on a 296-node sample, forces 34.8 against 27.9 s.)
+int sweep_rows(const sqb_ctx *c) {
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  auto fits = [&](int ry) {
+    return sweep_rows_supported(c->n, ry) && sweep_smem(c->n, c->lay_pmax, c->n_gproj, ry) <= (size_t)optin;
+  };
+  if (c->sweep_ry && fits(c->sweep_ry)) return c->sweep_ry;
+  return 2;
+}
+
 // The context's part of a sweep-kernel launch (grid, fields, replicas, queue).
 void fill_sweep_args(sqb_ctx *c, const int *d_list, int count, size_t stride, SweepArgs &s) {
   std::memset(&s, 0, sizeof(s));
@@ -418,7 +435,8 @@ void fill_sweep_args(sqb_ctx *c, const int *d_list, int count, size_t stride, Sw
   s.status = c->d_status;
   s.scratch = c->d_scratch;
   s.scratch_stride = stride;
-  s.nsweep = sweep_threads(c->n);
+  s.ry = sweep_rows(c);
+  s.nsweep = sweep_threads(c->n, s.ry);
   s.proj_points = c->d_proj_points;
 }
 
@@ -1328,6 +1346,14 @@ static int spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, doubl
   return sqb_density_energy(c, lam, rho, ci, ebs, eent);
 }
 
+int sqb_set_sweep_rows(sqb_ctx *c, int rows) {
+  if (!c || (rows != 0 && rows != 2 && rows != 3)) return SQB_ERR_ARG;
+  if (rows == 3 && !sweep_rows_supported(c->n, 3)) return SQB_ERR_UNSUPPORTED;
+  c->sweep_ry = rows;
+  drop_graph(c);
+  return SQB_OK;
+}
+
 int sqb_test_stage_wait(sqb_ctx *c, unsigned extra_bytes, double wait_ms) {
   if (!c || !(wait_ms >= 0.0) || wait_ms > 10000.0 || extra_bytes % 16 != 0 || extra_bytes > 4096u)
     return SQB_ERR_ARG;
@@ -1414,6 +1440,67 @@ int sqb_autotune(sqb_ctx *c, int sample, int *chosen, double *ms_out) {
   if (chosen) *chosen = c->cols;
   if (ms_out)
     for (int k = 0; k < 3; k++) ms_out[k] = ms[k];
+  return SQB_OK;
+}
+
+int sqb_autotune_sweep(sqb_ctx *c, int sample, int *rows, double *ms_out) {
+  if (!c || sample < 0) return SQB_ERR_ARG;
+  if (!c->have_veff || !c->have_atoms || !c->have_proj) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  bool sw = false;
+  int rc = use_sweep(c, &sw);
+  if (rc) return rc;
+  if (!sw) return SQB_ERR_UNSUPPORTED;
+  const int N = c->nnode;
+  int count = sample > 0 ? sample : 2 * c->sms;
+  if (count > N) count = N;
+  std::vector<int> list(count);
+  for (int i = 0; i < count; i++) list[i] = (int)((long long)i * N / count);  // evenly spaced nodes
+  rc = ensure_tmp(c, (size_t)count * sizeof(int));
+  if (rc) return rc;
+  int *d_list = reinterpret_cast<int *>(c->d_tmp);
+  CK(cudaMemcpy(d_list, list.data(), (size_t)count * sizeof(int), cudaMemcpyHostToDevice));
+  const int keep = c->sweep_ry;
+  double ms[2] = {-1.0, -1.0};
+  int best = 0;
+  for (int k = 0; k < 2; k++) {
+    c->sweep_ry = 2 + k;
+    if (sweep_rows(c) != c->sweep_ry) continue;  // not covered for this window
+    NodeArgs a;
+    fill_node_args(c, a);
+    a.mode = MODE_SQ;
+    a.chi = c->d_chi;
+    a.zee = c->d_zee;
+    a.rho_pj = c->d_rho_pj;
+    a.lmin = c->d_lmin;
+    a.lmax = c->d_lmax;
+    a.lanczos_iters = c->d_iters;
+    float t = 0.f;
+    for (int rep = 0; rep < 2; rep++) {  // the first launch of a variant is a warm-up
+      CK(cudaEventRecord(c->ev0, c->stream));
+      rc = run_sq_nodes(c, a, d_list, count);
+      if (!rc) {
+        CK(cudaEventRecord(c->ev1, c->stream));
+        rc = read_status(c);
+      }
+      if (rc) {
+        c->sweep_ry = keep;
+        return rc;
+      }
+      t = elapsed(c);
+    }
+    ms[k] = t;
+    if (ms[best] < 0.0 || ms[k] < ms[best]) best = k;
+  }
+  c->sweep_ry = 2 + best;
+  drop_graph(c);
+  c->have_moments = false;  // the sample runs overwrote part of the per-node outputs
+  c->have_ci = false;
+  if (rows) *rows = c->sweep_ry;
+  if (ms_out) {
+    ms_out[0] = ms[0];
+    ms_out[1] = ms[1];
+  }
   return SQB_OK;
 }
 

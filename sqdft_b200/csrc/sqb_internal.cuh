@@ -144,6 +144,7 @@ struct SweepArgs {
   unsigned char *scratch;
   size_t scratch_stride;  // bytes per CTA: three window vectors (FP64), then the flush buffer
   int nsweep;             // threads of the block (a multiple of 32)
+  int ry;                 // window rows per thread (2, or 3 up to 33-wide windows)
   double *chi, *zee, *rho_pj, *lmin, *lmax;
   int *lanczos_iters;
   // ForcesNonLocal (sweep_force_kernel): bounds in chi, zee (inputs), the
@@ -157,9 +158,10 @@ struct SweepArgs {
   unsigned long long *proj_points;  // [3]: ball points x steps (all, Chebyshev only), ball-in-window points x steps
 };
 
-// Sweep kernel launchers (sqb_sweep.cu).
-int sweep_threads(int n);
-size_t sweep_smem(int n, int pmax, int n_gproj);
+// Sweep kernel launchers (sqb_sweep.cu); ry: window rows per thread.
+int sweep_threads(int n, int ry);
+size_t sweep_smem(int n, int pmax, int n_gproj, int ry);
+bool sweep_rows_supported(int n, int ry);
 size_t sweep_scratch_bytes(int n, int pmax);  // scratch per CTA
 cudaError_t sweep_setup(int n);
 cudaError_t launch_sweep(const SweepArgs &a, int grid, cudaStream_t s);

@@ -38,21 +38,27 @@ __global__ void fill_empty_kernel(unsigned long long *lay_id, long long evol, un
 }
 
 // Launch bounds of the instantiations (the register budget per thread is
-// set by the warps per SM sub-partition): windows up to 31 wide run 512
-// threads (16 warps, 128 registers), 33 wide 576 (96), up to 43 wide 1024.
-constexpr int MAXT_A = 512, MAXT_B = 576, MAXT_C = 1024;
+// set by the warps per SM sub-partition).  Two rows per thread: windows up
+// to 31 wide run 512 threads (16 warps, 128 registers), 33 wide 576 (96), up
+// to 43 wide 1024.  Three rows per thread: up to 33 wide, 384 threads (12
+// warps, 168 registers), for fields whose many dot-product accumulators
+// spill at the smaller budgets.
+constexpr int MAXT_A = 512, MAXT_B = 576, MAXT_C = 1024, MAXT_R3 = 384;
 
-template <int PM, int FORM, int MAXT>
+template <int PM, int FORM, int MAXT, int RY>
 cudaError_t set_attr(size_t smem) {
-  return cudaFuncSetAttribute(sweep::sweep_kernel<PM, FORM, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(sweep::sweep_kernel<PM, FORM, MAXT, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem);
 }
 
 template <int PM, int FORM>
 cudaError_t launch_form(const SweepArgs &a, int grid, int threads, size_t smem, cudaStream_t s) {
-  if (threads <= MAXT_A) sweep::sweep_kernel<PM, FORM, MAXT_A><<<grid, threads, smem, s>>>(a);
-  else if (threads <= MAXT_B) sweep::sweep_kernel<PM, FORM, MAXT_B><<<grid, threads, smem, s>>>(a);
-  else if (threads <= MAXT_C) sweep::sweep_kernel<PM, FORM, MAXT_C><<<grid, threads, smem, s>>>(a);
+  if (a.ry == 3) {
+    if (threads > MAXT_R3) return cudaErrorInvalidConfiguration;
+    sweep::sweep_kernel<PM, FORM, MAXT_R3, 3><<<grid, threads, smem, s>>>(a);
+  } else if (threads <= MAXT_A) sweep::sweep_kernel<PM, FORM, MAXT_A, 2><<<grid, threads, smem, s>>>(a);
+  else if (threads <= MAXT_B) sweep::sweep_kernel<PM, FORM, MAXT_B, 2><<<grid, threads, smem, s>>>(a);
+  else if (threads <= MAXT_C) sweep::sweep_kernel<PM, FORM, MAXT_C, 2><<<grid, threads, smem, s>>>(a);
   else return cudaErrorInvalidConfiguration;
   return cudaGetLastError();
 }
@@ -66,9 +72,12 @@ cudaError_t launch_pm(const SweepArgs &a, int grid, int threads, size_t smem, cu
 
 template <int PM>
 cudaError_t setup_pm(size_t smem) {
-  cudaError_t r[9] = {set_attr<PM, 0, MAXT_A>(smem), set_attr<PM, 1, MAXT_A>(smem), set_attr<PM, 2, MAXT_A>(smem),
-                      set_attr<PM, 0, MAXT_B>(smem), set_attr<PM, 1, MAXT_B>(smem), set_attr<PM, 2, MAXT_B>(smem),
-                      set_attr<PM, 0, MAXT_C>(smem), set_attr<PM, 1, MAXT_C>(smem), set_attr<PM, 2, MAXT_C>(smem)};
+  cudaError_t r[12] = {set_attr<PM, 0, MAXT_A, 2>(smem),  set_attr<PM, 1, MAXT_A, 2>(smem),
+                       set_attr<PM, 2, MAXT_A, 2>(smem),  set_attr<PM, 0, MAXT_B, 2>(smem),
+                       set_attr<PM, 1, MAXT_B, 2>(smem),  set_attr<PM, 2, MAXT_B, 2>(smem),
+                       set_attr<PM, 0, MAXT_C, 2>(smem),  set_attr<PM, 1, MAXT_C, 2>(smem),
+                       set_attr<PM, 2, MAXT_C, 2>(smem),  set_attr<PM, 0, MAXT_R3, 3>(smem),
+                       set_attr<PM, 1, MAXT_R3, 3>(smem), set_attr<PM, 2, MAXT_R3, 3>(smem)};
   for (cudaError_t e : r)
     if (e != cudaSuccess) return e;
   return cudaSuccess;
@@ -76,12 +85,18 @@ cudaError_t setup_pm(size_t smem) {
 
 }  // namespace
 
-int sweep_threads(int n) { return sweep::sweep_threads_of(n); }
+int sweep_threads(int n, int ry) { return sweep::sweep_threads_of(n, ry); }
 
-size_t sweep_smem(int n, int pmax, int n_gproj) {
-  const int nt = sweep::sweep_threads_of(n);
-  return sweep::shared_fixed() + sweep::planes_bytes(n) + sweep::ring_bytes(nt, pmax) + sweep::accw_bytes(nt, pmax) +
-         (((size_t)(n_gproj + pmax) * sizeof(double) + 127) & ~size_t(127));
+bool sweep_rows_supported(int n, int ry) {
+  if (ry == 2) return sweep::sweep_threads_of(n, 2) <= MAXT_C;
+  if (ry == 3) return sweep::sweep_threads_of(n, 3) <= MAXT_R3;
+  return false;
+}
+
+size_t sweep_smem(int n, int pmax, int n_gproj, int ry) {
+  const int nt = sweep::sweep_threads_of(n, ry);
+  return sweep::shared_fixed() + sweep::planes_bytes(n, ry) + sweep::ring_bytes(nt, pmax, ry) +
+         sweep::accw_bytes(nt, pmax, ry) + (((size_t)(n_gproj + pmax) * sizeof(double) + 127) & ~size_t(127));
 }
 
 size_t sweep_scratch_bytes(int n, int pmax) {
@@ -101,9 +116,9 @@ cudaError_t sweep_setup(int n) {
 }
 
 cudaError_t launch_sweep(const SweepArgs &a, int grid, cudaStream_t s) {
-  const int threads = sweep_threads(a.n);
-  if (a.n > MAXN || threads > MAXT_C) return cudaErrorInvalidConfiguration;
-  const size_t smem = sweep_smem(a.n, a.pmax, a.n_gproj);
+  const int threads = sweep_threads(a.n, a.ry);
+  if (a.n > MAXN || !sweep_rows_supported(a.n, a.ry) || threads != a.nsweep) return cudaErrorInvalidConfiguration;
+  const size_t smem = sweep_smem(a.n, a.pmax, a.n_gproj, a.ry);
   if (a.pmax == 1) return launch_pm<1>(a, grid, threads, smem, s);
   if (a.pmax == 3) return launch_pm<3>(a, grid, threads, smem, s);
   return cudaErrorInvalidValue;

@@ -45,7 +45,7 @@ namespace sqb {
 namespace sweep {
 
 constexpr int KL = LAYERS;
-constexpr int RY = 2;  // window rows per thread
+constexpr int RY_DEFAULT = 2;  // window rows per thread (3 for fields with three projectors per slot)
 
 // Sweep kinds: the Lanczos start vector's projections only; a Lanczos step;
 // a Chebyshev step; a Chebyshev step that also accumulates the density-matrix
@@ -86,12 +86,12 @@ struct Shared {
 };
 
 __host__ __device__ constexpr int plane_pitch(int n) { return n + 2 * FDN; }
-// two halo'd planes, plus one row of slack: the shared y-arm loads of a row
-// pair whose second row lies beyond the window read one row past the plane
-// (into values that are not used)
-__host__ __device__ inline size_t planes_bytes(int n) {
+// two halo'd planes, plus ry - 1 rows of slack: the shared y-arm loads of a
+// row group whose last rows lie beyond the window read up to ry - 1 rows past
+// the plane (into values that are not used)
+__host__ __device__ inline size_t planes_bytes(int n, int ry) {
   const int P = plane_pitch(n);
-  return ((size_t)(2 * P * P + P + 8) * sizeof(double) + 127) & ~size_t(127);
+  return ((size_t)(2 * P * P + (ry - 1) * P + 8) * sizeof(double) + 127) & ~size_t(127);
 }
 // Lanczos sweeps of the one-projector fields also accumulate the dot products
 // of their input (the exact chi^T W_m, see lanczos), flushed into a second
@@ -105,16 +105,16 @@ __host__ __device__ inline size_t shared_fixed() { return (sizeof(Shared) + 127)
 // The threads' rings of the FDN planes behind (RSLOT slots, sized for FP64).
 constexpr int RSLOT = 8;
 __host__ __device__ constexpr bool uses_ring(int pm) { return pm >= 1; }
-__host__ __device__ inline size_t ring_bytes(int nsweep, int pm) {
-  return uses_ring(pm) ? (((size_t)RSLOT * RY * nsweep * sizeof(double) + 127) & ~size_t(127)) : 0;
+__host__ __device__ inline size_t ring_bytes(int nsweep, int pm, int ry) {
+  return uses_ring(pm) ? (((size_t)RSLOT * ry * nsweep * sizeof(double) + 127) & ~size_t(127)) : 0;
 }
 // Lanczos sweeps' input-dot partials, one slot per (layer, row, thread): the
 // owning thread accumulates, flushes and clears its own slots.
-__host__ __device__ inline size_t accw_bytes(int nsweep, int pm) {
-  return input_dots(pm) ? (((size_t)KL * RY * nsweep * sizeof(double) + 127) & ~size_t(127)) : 0;
+__host__ __device__ inline size_t accw_bytes(int nsweep, int pm, int ry) {
+  return input_dots(pm) ? (((size_t)KL * ry * nsweep * sizeof(double) + 127) & ~size_t(127)) : 0;
 }
-__host__ __device__ inline int sweep_threads_of(int n) {
-  const int cols = n * ((n + RY - 1) / RY);
+__host__ __device__ inline int sweep_threads_of(int n, int ry) {
+  const int cols = n * ((n + ry - 1) / ry);
   const int t = ((cols + 31) / 32) * 32;
   return t < 64 ? 64 : t;  // two warps at least: the multisection's two extremes
 }
@@ -196,7 +196,7 @@ __device__ __forceinline__ void reduce_instance(const SweepArgs &a, Shared &S, c
 // the FDN planes behind in the thread's own slots of a shared ring (plane
 // z - s in slot (z - s) mod RSLOT); without it, all 2 FDN + 1 planes in
 // registers (fut[j][FDN + s] plane z + s).
-template <typename T, int PM, int SK>
+template <typename T, int PM, int SK, int RY>
 __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned char *dyn, const IO<T> &io,
                                       double &acc0, double &acc1) {
   constexpr bool STENCIL = SK != SK_ONES;
@@ -216,10 +216,10 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   const unsigned dummy = (unsigned)a.n_gproj;
   const unsigned long long empty = 0x0001000100010001ull * (unsigned long long)dummy;  // no ball in any layer
   T *sm = reinterpret_cast<T *>(dyn);
-  T *ring = reinterpret_cast<T *>(dyn + planes_bytes(n));
-  double *accw = reinterpret_cast<double *>(dyn + planes_bytes(n) + ring_bytes(NS, PM));
+  T *ring = reinterpret_cast<T *>(dyn + planes_bytes(n, RY));
+  double *accw = reinterpret_cast<double *>(dyn + planes_bytes(n, RY) + ring_bytes(NS, PM, RY));
   const double *pcur =
-      reinterpret_cast<const double *>(dyn + planes_bytes(n) + ring_bytes(NS, PM) + accw_bytes(NS, PM));
+      reinterpret_cast<const double *>(dyn + planes_bytes(n, RY) + ring_bytes(NS, PM, RY) + accw_bytes(NS, PM, RY));
   double *fb = slot<double>(a, 3);                // flush buffer: [set][layer][projector][plane][column]
   double *fbw = fb + (size_t)KL * PM * n * n2;  // IND: the input's set
   const double *veff = a.veff64;
@@ -347,23 +347,45 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
       if constexpr (STENCIL) {
         // arm k of each point sums (x-k) + (x+k) + (y-k) + (y+k) + (z-k) + (z+k)
         // in that order before the coefficient, as HsubTimesVec does
-        // (sq.cpp:894-897); rows y0-k and y0+1+k are loaded once for both rows
-        const T *c0p = smz + (yb + FDN) * P + x + FDN;
-        const T *c1p = c0p + P;
+        // (sq.cpp:894-897).  The RY rows y0..y0+RY-1 of a thread share their
+        // y-arm loads: arm k loads rows y0-k (ym[k]) and y0+RY-1+k (yp[k]); row
+        // j's y0+j-k is the centre of row j-k when j >= k, else ym[k-j], and
+        // its y0+j+k the centre of row j+k when j+k < RY, else yp[j+k-RY+1].
+        const T *cp0 = smz + (yb + FDN) * P + x + FDN;
         double temp[RY];
 #pragma unroll
         for (int j = 0; j < RY; j++) temp[j] = (double)fut[j][C] * c0;
-        T prev_m = fut[0][C], prev_p = fut[1][C];
+        if constexpr (RY == 2) {
+          // the same, with the loads of the previous arm carried in two registers
+          const T *c1p = cp0 + P;
+          T prev_m = fut[0][C], prev_p = fut[1][C];
 #pragma unroll
-        for (int k = 1; k <= FDN; k++) {
-          const T ym = c0p[-k * P], yp = c1p[k * P];
-          const T zm0 = RING ? rslot(0, z - k) : fut[0][C - k], zm1 = RING ? rslot(1, z - k) : fut[1][C - k];
-          const T s0 = c0p[-k] + c0p[k] + ym + prev_p + zm0 + fut[0][C + k];
-          const T s1 = c1p[-k] + c1p[k] + prev_m + yp + zm1 + fut[1][C + k];
-          temp[0] += (double)s0 * a.coeff_lap[k];
-          temp[1] += (double)s1 * a.coeff_lap[k];
-          prev_m = ym;
-          prev_p = yp;
+          for (int k = 1; k <= FDN; k++) {
+            const T ym = cp0[-k * P], yp = c1p[k * P];
+            const T zm0 = RING ? rslot(0, z - k) : fut[0][C - k], zm1 = RING ? rslot(1, z - k) : fut[1][C - k];
+            const T s0 = cp0[-k] + cp0[k] + ym + prev_p + zm0 + fut[0][C + k];
+            const T s1 = c1p[-k] + c1p[k] + prev_m + yp + zm1 + fut[1][C + k];
+            temp[0] += (double)s0 * a.coeff_lap[k];
+            temp[1] += (double)s1 * a.coeff_lap[k];
+            prev_m = ym;
+            prev_p = yp;
+          }
+        } else {
+          T ym[FDN + 1], yp[FDN + 1];
+#pragma unroll
+          for (int k = 1; k <= FDN; k++) {
+            ym[k] = cp0[-k * P];
+            yp[k] = cp0[(RY - 1 + k) * P];
+#pragma unroll
+            for (int j = 0; j < RY; j++) {
+              const T *cj = cp0 + j * P;
+              const T ylo = j >= k ? fut[j - k][C] : ym[k - j];
+              const T yhi = j + k < RY ? fut[j + k][C] : yp[j + k - RY + 1];
+              const T zm = RING ? rslot(j, z - k) : fut[j][C - k];
+              const T sj = cj[-k] + cj[k] + ylo + yhi + zm + fut[j][C + k];
+              temp[j] += (double)sj * a.coeff_lap[k];
+            }
+          }
         }
 #pragma unroll
         for (int j = 0; j < RY; j++) {
@@ -751,7 +773,7 @@ static __device__ void count_proj_points(const SweepArgs &a, Shared &S, long lon
 // extremes moved by no more than the tolerance, at most 500 steps) applies.
 // The projections chi^T W_m+1 the next gather needs follow from the recurrence
 // on the dot products of the sweep's output.
-template <typename T, int PM, bool LQ>
+template <typename T, int PM, bool LQ, int RY>
 __device__ void lanczos(const SweepArgs &a, Shared &S, unsigned char *dyn, double *pcur, double &lmin_out,
                         double &lmax_out, int &rows_out) {
   const int tid = threadIdx.x;
@@ -769,7 +791,7 @@ __device__ void lanczos(const SweepArgs &a, Shared &S, unsigned char *dyn, doubl
     // with chk = 0)
     IO<T> io;
     io.chk = chk;
-    sweep<T, PM, SK_ONES>(a, S, dyn, io, d0, d1);
+    sweep<T, PM, SK_ONES, RY>(a, S, dyn, io, d0, d1);
     __syncthreads();
     for (int p = tid; p < S.n_pi; p += blockDim.x) {
       S.pw_cur[p] = s0 * S.p_nxt[p];
@@ -803,7 +825,7 @@ __device__ void lanczos(const SweepArgs &a, Shared &S, unsigned char *dyn, doubl
     }
     d0 = 0.0;
     d1 = 0.0;
-    sweep<T, PM, SK_LZF>(a, S, dyn, io, d0, d1);
+    sweep<T, PM, SK_LZF, RY>(a, S, dyn, io, d0, d1);
     sweep_sum2(S, d0, d1, a.nsweep);
     // b_m-1 = |W_m| and a_m = <W_m, H W_m> / b_m-1^2 (W_0 is normalised)
     const double bm = m == 0 ? 1.0 : sqrt(S.scal[0]);
@@ -867,7 +889,7 @@ __device__ void lanczos(const SweepArgs &a, Shared &S, unsigned char *dyn, doubl
 }
 
 // Chebyshev moments mu_j = e_c^T T_j((H - chi)/zee) e_c / h^3 (sq.cpp:564-655).
-template <int PM>
+template <int PM, int RY>
 __device__ void moments(const SweepArgs &a, Shared &S, unsigned char *dyn, double *pcur, double chi, double zee,
                         double *mu) {
   double *B0 = slot<double>(a, 0), *B1 = slot<double>(a, 1);
@@ -880,7 +902,7 @@ __device__ void moments(const SweepArgs &a, Shared &S, unsigned char *dyn, doubl
     io.out = B1;
     io.ca = chi;
     io.cb = zee;
-    sweep<double, PM, SK_CH>(a, S, dyn, io, d0, d1);
+    sweep<double, PM, SK_CH, RY>(a, S, dyn, io, d0, d1);
   }
   __syncthreads();
   rotate(S, pcur);
@@ -903,7 +925,7 @@ __device__ void moments(const SweepArgs &a, Shared &S, unsigned char *dyn, doubl
       io.dbl = nq > q1;
       d0 = 0.0;
       d1 = 0.0;
-      sweep<double, PM, SK_CH>(a, S, dyn, io, d0, d1);
+      sweep<double, PM, SK_CH, RY>(a, S, dyn, io, d0, d1);
       if (nq > q1) sweep_sum2(S, d0, d1, a.nsweep);
     }
     __syncthreads();
@@ -956,7 +978,7 @@ static __device__ void sweep_sum3(Shared &S, double v0, double v1, double v2) {
 // of D (zero outside the window) contracted with the replica's projectors:
 // f = -4 h^3 sum_q (chi_q . grad D) chi_q(centre) / Denom_q, into the node's
 // force slots (atom, fx, fy, fz).
-template <typename T, int PM>
+template <typename T, int PM, int RY>
 __device__ void node_forces(const SweepArgs &a, Shared &S, unsigned char *dyn, double *pcur, double chi,
                             double zee, const double *ci, double *fslot) {
   T *B0 = slot<T>(a, 0), *B1 = slot<T>(a, 1);
@@ -973,7 +995,7 @@ __device__ void node_forces(const SweepArgs &a, Shared &S, unsigned char *dyn, d
     io.dacc = D;
     io.ce = ci[0];
     io.cd = ci[1];
-    sweep<T, PM, SK_FD>(a, S, dyn, io, d0, d1);
+    sweep<T, PM, SK_FD, RY>(a, S, dyn, io, d0, d1);
   }
   __syncthreads();
   rotate(S, pcur);
@@ -988,7 +1010,7 @@ __device__ void node_forces(const SweepArgs &a, Shared &S, unsigned char *dyn, d
     io.cb = zee;
     io.dacc = D;
     io.cd = ci[nq];
-    sweep<T, PM, SK_FD>(a, S, dyn, io, d0, d1);
+    sweep<T, PM, SK_FD, RY>(a, S, dyn, io, d0, d1);
     __syncthreads();
     rotate(S, pcur);
     T *tt = t0;
@@ -1051,13 +1073,13 @@ __device__ void node_forces(const SweepArgs &a, Shared &S, unsigned char *dyn, d
 }
 
 // The force pass over the listed nodes (bounds from chi, zee; Ci from ci).
-template <int PM, typename T, int MAXT>
+template <int PM, typename T, int MAXT, int RY>
 __global__ void __launch_bounds__(MAXT, 1) sweep_force_kernel(SweepArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   Shared &S = *reinterpret_cast<Shared *>(smem);
   unsigned char *dyn = smem + shared_fixed();
   double *pcur =
-      reinterpret_cast<double *>(dyn + planes_bytes(a.n) + ring_bytes(a.nsweep, PM) + accw_bytes(a.nsweep, PM));
+      reinterpret_cast<double *>(dyn + planes_bytes(a.n, RY) + ring_bytes(a.nsweep, PM, RY) + accw_bytes(a.nsweep, PM, RY));
   for (int i = threadIdx.x; i < a.n_gproj + PM; i += blockDim.x) pcur[i] = 0.0;  // [n_gproj..]: the empty id
   for (;;) {
     if (threadIdx.x == 0) {
@@ -1076,7 +1098,7 @@ __global__ void __launch_bounds__(MAXT, 1) sweep_force_kernel(SweepArgs a) {
     double *fs = a.fslots + (size_t)S.qidx * FSLOTS * 4;
     for (int i = threadIdx.x; i < FSLOTS * 4; i += blockDim.x) fs[i] = (i % 4 == 0) ? -1.0 : 0.0;
     setup_node(a, S);
-    node_forces<T, PM>(a, S, dyn, pcur, a.chi[node], a.zee[node], a.ci + (size_t)node * (a.npl + 1), fs);
+    node_forces<T, PM, RY>(a, S, dyn, pcur, a.chi[node], a.zee[node], a.ci + (size_t)node * (a.npl + 1), fs);
     __syncthreads();
   }
 }
@@ -1115,13 +1137,13 @@ static __device__ void quadrature_moments(const SweepArgs &a, Shared &S, int k, 
 
 // FORM: 0 FP64, 1 FP32-mixed, 2 Lanczos quadrature.  MAXT bounds the block,
 // which sets the register budget per thread.
-template <int PM, int FORM, int MAXT>
+template <int PM, int FORM, int MAXT, int RY>
 __global__ void __launch_bounds__(MAXT, 1) sweep_kernel(SweepArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   Shared &S = *reinterpret_cast<Shared *>(smem);
   unsigned char *dyn = smem + shared_fixed();
   double *pcur =
-      reinterpret_cast<double *>(dyn + planes_bytes(a.n) + ring_bytes(a.nsweep, PM) + accw_bytes(a.nsweep, PM));
+      reinterpret_cast<double *>(dyn + planes_bytes(a.n, RY) + ring_bytes(a.nsweep, PM, RY) + accw_bytes(a.nsweep, PM, RY));
   for (int i = threadIdx.x; i < a.n_gproj + PM; i += blockDim.x) pcur[i] = 0.0;  // [n_gproj..]: the empty id
   for (;;) {
     if (threadIdx.x == 0) {
@@ -1142,7 +1164,7 @@ __global__ void __launch_bounds__(MAXT, 1) sweep_kernel(SweepArgs a) {
     int rows = 0;
     double *mu = a.rho_pj + (size_t)node * (a.npl + 1);
     if constexpr (FORM == 2) {
-      lanczos<double, PM, true>(a, S, dyn, pcur, lmin, lmax, rows);
+      lanczos<double, PM, true, RY>(a, S, dyn, pcur, lmin, lmax, rows);
       const double chi = 0.5 * (lmax + lmin), zee = 0.5 * (lmax - lmin);
       if ((long long)rows <= (long long)a.n * a.n * a.n) quadrature_moments(a, S, rows, chi, zee, mu);
       else if (threadIdx.x == 0) atomicOr(a.status, ST_CAPACITY);
@@ -1150,12 +1172,12 @@ __global__ void __launch_bounds__(MAXT, 1) sweep_kernel(SweepArgs a) {
       rows -= 1;  // reported as Lanczos iterations: matvecs = iterations + 1
     } else {
       using TL = typename std::conditional<FORM == 1, float, double>::type;
-      lanczos<TL, PM, false>(a, S, dyn, pcur, lmin, lmax, rows);
+      lanczos<TL, PM, false, RY>(a, S, dyn, pcur, lmin, lmax, rows);
       const double chi = (lmax + lmin) / 2, zee = (lmax - lmin) / 2;  // sq.cpp:564-565
       count_proj_points(a, S, rows + 1, 0);
       // moments stay FP64 in both forms: FP32 storage of the Chebyshev vectors
       // grows a rounding error injected at step i like (k - i) by step k
-      moments<PM>(a, S, dyn, pcur, chi, zee, mu);
+      moments<PM, RY>(a, S, dyn, pcur, chi, zee, mu);
       count_proj_points(a, S, a.npl / 2, 1);
     }
     if (threadIdx.x == 0) {

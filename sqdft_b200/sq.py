@@ -40,7 +40,7 @@ EXPORTS = [
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
     "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check", "sqb_lanczos_moments_nodes",
     "sqb_set_node_kernel", "sqb_set_veff_device", "sqb_test_stage_wait", "sqb_density_loss",
-    "sqb_density_loss_vjp",
+    "sqb_density_loss_vjp", "sqb_set_sweep_rows", "sqb_autotune_sweep",
 ]
 
 
@@ -115,6 +115,8 @@ def library() -> C.CDLL:
         lib.sqb_set_veff_device.argtypes = [P, C.c_void_p]
         lib.sqb_test_stage_wait.argtypes = [P, C.c_uint, C.c_double]
         lib.sqb_density_loss.argtypes = [P, _dp, _dp]
+        lib.sqb_set_sweep_rows.argtypes = [P, C.c_int]
+        lib.sqb_autotune_sweep.argtypes = [P, C.c_int, _ip, _dp]
         lib.sqb_density_loss_vjp.argtypes = [P, _dp, C.c_int, C.c_double, _dp, _dp]
         lib.sqb_moments_vjp.argtypes = [P, _dp, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
@@ -239,6 +241,17 @@ class Context:
         if v.size != int(np.prod(self._veff_ext_shape())):
             raise ValueError(f"Veff with halo must have shape {self._veff_ext_shape()}, got {v.shape}")
         _check(self.lib.sqb_set_veff(self.ptr, _d(v)), "sqb_set_veff")
+
+    def set_sweep_rows(self, rows: int = 0):
+        """sqb_set_sweep_rows: window rows per sweep-kernel thread (0 automatic, 2, 3)."""
+        _check(self.lib.sqb_set_sweep_rows(self.ptr, int(rows)), "sqb_set_sweep_rows")
+
+    def autotune_sweep(self, sample: int = 0):
+        """sqb_autotune_sweep: (rows chosen, [ms with 2 rows, ms with 3 rows])."""
+        rows = C.c_int()
+        ms = np.zeros(2)
+        _check(self.lib.sqb_autotune_sweep(self.ptr, int(sample), C.byref(rows), _d(ms)), "sqb_autotune_sweep")
+        return rows.value, ms
 
     def density_loss(self, w: np.ndarray) -> float:
         """sqb_density_loss: sum_p w_p rho_p of the last density."""

@@ -363,3 +363,29 @@ def test_sweep_kernel_forces_match_plane_kernel(golden, name, precision):
     assert np.abs(f_sweep - f_plane).max() <= (1e-12 if precision == 0 else 1e-9)
     if precision == 0:
         assert np.abs(f_sweep - ref["fnloc"]).max() <= 1e-7
+
+
+@pytest.mark.parametrize("name", ["tiny", "lihs"])
+def test_sweep_rows_give_the_same_results(golden, name):
+    """Two or three window rows per sweep-kernel thread (sqb_set_sweep_rows)
+    change only the summation order of the block reductions: bounds, moments
+    and forces agree to rounding, and the autotuner keeps one of the two."""
+    from sqdft_b200 import sq
+
+    case, ref = golden(name)
+    res = {}
+    with _ctx(case) as ctx:
+        for rows in (2, 3):
+            ctx.set_sweep_rows(rows)
+            out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+            res[rows] = (out, ctx.forces_nonlocal())
+            assert ctx.stats()["node_kernel"] == sq.SQB_KERNEL_SWEEP
+        rows, ms = ctx.autotune_sweep()
+        assert rows in (2, 3) and ms.min() > 0.0
+    (a, fa), (b, fb) = res[2], res[3]
+    for k in ("chi", "zee"):
+        assert np.abs(a[k] - b[k]).max() <= 1e-11
+    assert np.abs(a["rho_pj"] - b["rho_pj"]).max() <= 1e-11 * np.abs(a["rho_pj"]).max()
+    assert np.abs(a["rho"] - b["rho"]).max() <= 1e-11
+    assert np.abs(fa - fb).max() <= 1e-12
+    assert np.abs(b["rho"].ravel() - ref["rho"].ravel()).max() <= 1e-10
