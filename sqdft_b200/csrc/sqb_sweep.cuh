@@ -114,8 +114,8 @@ __host__ __device__ inline size_t accw_bytes(int nsweep, int pm, int ry) {
   return input_dots(pm) ? (((size_t)KL * ry * nsweep * sizeof(double) + 127) & ~size_t(127)) : 0;
 }
 __host__ __device__ inline int sweep_threads_of(int n, int ry) {
-  const int cols = n * ((n + ry - 1) / ry);
-  const int t = ((cols + 31) / 32) * 32;
+  const int groups = (n + ry - 1) / ry;
+  const int t = n <= 32 ? 32 * groups : ((n * groups + 31) / 32) * 32;  // see the thread mapping in sweep
   return t < 64 ? 64 : t;  // two warps at least: the multisection's two extremes
 }
 
@@ -208,9 +208,15 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   constexpr bool IND = SK == SK_LZF && input_dots(PM);  // dot products of the input too
   const int n = a.n, n2 = n * n, P = plane_pitch(n), P2 = P * P;
   const int tid = threadIdx.x, NS = a.nsweep, lane = tid & 31, warp = tid >> 5, nwarp = NS >> 5;
+  // thread -> (column x, row group): windows up to 32 wide give each row
+  // group a warp of its own (lane = column), so no warp straddles two row
+  // groups and its shared-plane loads are one contiguous run (no bank
+  // conflicts); wider windows pack the columns densely
   const int nrow = (n + RY - 1) / RY;
-  const bool tv = tid < n * nrow;
-  const int x = tv ? tid % n : 0, yb = tv ? (tid / n) * RY : 0;
+  const bool lanes = n <= 32;
+  const int tx = lanes ? (tid & 31) : tid % n, tg = lanes ? (tid >> 5) : tid / n;
+  const bool tv = tx < n && tg < nrow;
+  const int x = tv ? tx : 0, yb = tv ? tg * RY : 0;
   const int nl = a.nloc, gc = (nl * n + nl) * n + nl;  // window index of the centre
   const int EP = a.ex * a.ey, EV = (int)a.evol;  // the extended grid fits 32-bit indices
   const unsigned dummy = (unsigned)a.n_gproj;
