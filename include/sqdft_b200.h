@@ -203,13 +203,21 @@ int sqb_autotune_sweep(sqb_ctx *ctx, int sample, int *rows, double *ms);
  * turns the hook off.  No counterpart in the reference. */
 int sqb_test_stage_wait(sqb_ctx *ctx, unsigned extra_bytes, double wait_ms);
 
-/* CUDA-graph replay of the node-kernel sequence of sqb_lanczos_moments (and
- * so of the SQ step): work-queue and status resets, the persistent Lanczos +
- * Chebyshev launch and the bound min/max, captured on the first call after
- * a plain run has allocated their buffers and replayed afterwards; dropped
- * when atoms, launch layout or precision change.  The Fermi-level solve stays
- * host-driven (one launch per Brent or Newton trial, as the reference's
- * control flow).  on: 1 = use, 0 = plain launches (default). */
+/* CUDA-graph replay.  on = 1: the node-kernel sequence of
+ * sqb_lanczos_moments (work-queue and status resets, the persistent Lanczos +
+ * Chebyshev launch and the bound min/max), captured on the first call after
+ * a plain run has allocated their buffers and replayed afterwards; the
+ * Fermi-level solve stays host-driven (one launch per Brent or Newton trial).
+ * on = 2: in addition sqb_spectral_quadrature runs the whole step as one
+ * graph -- node kernel, min/max, the Fermi solve as a conditional while node
+ * (NeConstraint, then a one-thread step of Brent's or Newton's method, the
+ * host solvers' control flow and arithmetic, which sets the loop condition;
+ * at most 512 evaluations) and the density assembly -- with one launch and
+ * one synchronisation per step; single rank (no allreduce hook), sweep kernel
+ * and no active defect check, else the plain path runs.  In graph mode 2 the
+ * step's whole device time is reported in sqb_stats.ms_lanczos_moments.
+ * Graphs are dropped when atoms, launch layout or precision change.
+ * 0 = plain launches (default). */
 int sqb_set_graph(sqb_ctx *ctx, int on);
 
 /* Autotuner of the node kernel's plane-loop layout: times the Lanczos +

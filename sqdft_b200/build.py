@@ -21,7 +21,10 @@ LIB = BUILD / "libsqdft_b200.so"
 INCLUDE = HERE.parent / "include"
 
 SOURCES = ["sqb_api.cu", "sqb_node.cu", "sqb_node_forces.cu", "sqb_node_vjp.cu", "sqb_node_mixed.cu", "sqb_node_lq.cu",
-           "sqb_fermi.cu", "sqb_sweep.cu", "sqb_sweep_forces.cu"]
+           "sqb_fermi.cu", "sqb_sweep.cu", "sqb_sweep_forces.cu", "sqb_fermi_dev.cu"]
+# Sources that need flags of their own: the device-side Fermi solver rounds
+# every operation as the host solver does (no multiply-add contraction).
+EXTRA = {"sqb_fermi_dev.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -41,7 +44,7 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> Path:
     for src in SOURCES:
         obj = BUILD / (Path(src).stem + ".o")
         cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-               f"-I{INCLUDE}", "-c", str(CSRC / src), "-o", str(obj)]
+               *EXTRA.get(src, []), f"-I{INCLUDE}", "-c", str(CSRC / src), "-o", str(obj)]
         if verbose_ptxas:
             cmd.insert(-4, "-Xptxas=-v")
         cmds.append(cmd)

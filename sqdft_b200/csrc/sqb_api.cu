@@ -34,6 +34,8 @@ struct sqb_ctx {
   int cols = 0, ctas_per_sm = 1;
   int use_graph = 0;                       // replay the node-kernel sequence from a CUDA graph
   cudaGraphExec_t sq_graph = nullptr;      // captured Lanczos+moments sequence (node kernel, min/max)
+  cudaGraphExec_t step_graph = nullptr;    // the whole SQ step (sqb_set_graph(ctx, 2))
+  FermiDev *d_fermi = nullptr;             // its device-side Fermi solver state
   int sq_graph_warm = 0;                   // a plain run has allocated what the sequence uses
   int n = 0, nnode = 0, ex = 0, ey = 0, ez = 0;
   double h3 = 0.0;
@@ -623,6 +625,34 @@ int newton(sqb_ctx *c, double lambda0, double *root, int *iters) {
   return std::isfinite(lnew) ? SQB_OK : SQB_ERR_NONFINITE;
 }
 
+// Lanczos counts and projector points of the last full SQ launch into the stats.
+int lanczos_stats(sqb_ctx *c, std::vector<int> &its) {
+  const size_t N = c->nnode;
+  its.resize(N);
+  CK(cudaMemcpy(its.data(), c->d_iters, N * sizeof(int), cudaMemcpyDeviceToHost));
+  unsigned long long pp[3] = {0, 0, 0};
+  CK(cudaMemcpy(pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
+  long long sum = 0;
+  int mx = 0;
+  for (size_t i = 0; i < N; i++) {
+    sum += its[i];
+    mx = std::max(mx, its[i]);
+  }
+  c->stats.lanczos_iters = sum;
+  c->stats.max_lanczos_iters = mx;
+  long long capped = 0;
+  // (the quadrature form reports rows - 1 iterations, so its cap shows as 499)
+  const int cap = LANCZOS_MAX_ITER - (c->precision == SQB_FP64_LANCZOS_QUAD ? 1 : 0);
+  for (size_t i = 0; i < N; i++) capped += its[i] >= cap;
+  c->stats.lanczos_maxiter_nodes = capped;
+  // passes: Lanczos 2 per iteration + 2, Chebyshev npl/2 (matvec passes only)
+  c->stats.matvecs = sum + (long long)N + (c->precision == SQB_FP64_LANCZOS_QUAD ? 0LL : (long long)N * (c->g.npl / 2));
+  c->stats.proj_points = (long long)pp[0];
+  c->stats.proj_points_cheb = (long long)pp[1];
+  c->stats.proj_points_window = (long long)pp[2];
+  return SQB_OK;
+}
+
 float elapsed(sqb_ctx *c) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -634,6 +664,8 @@ void drop_graph(sqb_ctx *c) {
   if (c->sq_graph) cudaGraphExecDestroy(c->sq_graph);
   c->sq_graph = nullptr;
   c->sq_graph_warm = 0;
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  c->step_graph = nullptr;
 }
 
 }  // namespace
@@ -741,7 +773,7 @@ int sqb_destroy(sqb_ctx *c) {
                   c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
                   c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
-                  c->d_f, c->d_tmp, c->d_sens, c->d_loss};
+                  c->d_f, c->d_tmp, c->d_sens, c->d_loss, c->d_fermi};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   drop_graph(c);
@@ -1072,28 +1104,9 @@ int sqb_lanczos_moments(sqb_ctx *c, double *chi, double *zee, double *rho_pj, in
   c->lmin_all = mm[0];
   c->lmax_all = mm[1];
   const size_t N = c->nnode, K = c->g.npl + 1;
-  std::vector<int> its(N);
-  CK(cudaMemcpy(its.data(), c->d_iters, N * sizeof(int), cudaMemcpyDeviceToHost));
-  unsigned long long pp[3] = {0, 0, 0};
-  CK(cudaMemcpy(pp, c->d_proj_points, sizeof(pp), cudaMemcpyDeviceToHost));
-  long long sum = 0;
-  int mx = 0;
-  for (size_t i = 0; i < N; i++) {
-    sum += its[i];
-    mx = std::max(mx, its[i]);
-  }
-  c->stats.lanczos_iters = sum;
-  c->stats.max_lanczos_iters = mx;
-  long long capped = 0;
-  // (the quadrature form reports rows - 1 iterations, so its cap shows as 499)
-  const int cap = LANCZOS_MAX_ITER - (c->precision == SQB_FP64_LANCZOS_QUAD ? 1 : 0);
-  for (size_t i = 0; i < N; i++) capped += its[i] >= cap;
-  c->stats.lanczos_maxiter_nodes = capped;
-  // passes: Lanczos 2 per iteration + 2, Chebyshev npl/2 (matvec passes only)
-  c->stats.matvecs = sum + (long long)N + (c->precision == SQB_FP64_LANCZOS_QUAD ? 0LL : (long long)N * (c->g.npl / 2));
-  c->stats.proj_points = (long long)pp[0];
-  c->stats.proj_points_cheb = (long long)pp[1];
-  c->stats.proj_points_window = (long long)pp[2];
+  std::vector<int> its;
+  rc = lanczos_stats(c, its);
+  if (rc) return rc;
   if (lanczos_iters) std::memcpy(lanczos_iters, its.data(), N * sizeof(int));
   if (chi) CK(cudaMemcpy(chi, c->d_chi, N * sizeof(double), cudaMemcpyDeviceToHost));
   if (zee) CK(cudaMemcpy(zee, c->d_zee, N * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1327,8 +1340,150 @@ int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *
   return rc;
 }
 
+// The whole SQ step as one CUDA graph (sqb_set_graph(ctx, 2)): the node
+// kernel and the bound min/max, the Fermi solve as a conditional while node
+// (NeConstraint, block sums, fermi_step) and the density assembly; one launch
+// and one synchronisation per step.  Single rank only (the reductions of
+// several ranks go through the host) and without the defect check.
+static int build_step_graph(sqb_ctx *c) {
+  if (!c->d_fermi) CK(cudaMalloc((void **)&c->d_fermi, sizeof(FermiDev)));
+  NodeArgs a;
+  fill_node_args(c, a);
+  a.mode = MODE_SQ;
+  a.chi = c->d_chi;
+  a.zee = c->d_zee;
+  a.rho_pj = c->d_rho_pj;
+  a.lmin = c->d_lmin;
+  a.lmax = c->d_lmax;
+  a.lanczos_iters = c->d_iters;
+  FermiArgs fa = fermi_args(c);
+  fa.lam_dev = &c->d_fermi->x;
+  FermiArgs fd = fermi_args(c);
+  fd.lam_dev = &c->d_fermi->root;
+  fd.status = &c->d_fermi->dstat;
+  const int deriv = c->g.fermi_alg == 2;
+  cudaGraph_t g = nullptr;
+  int rc = SQB_OK;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  rc = run_sq_nodes(c, a, c->d_nodes, c->nnode);
+  if (!rc && launch_minmax(c->d_lmin, c->d_lmax, c->nnode, c->d_result, c->stream) != cudaSuccess) rc = SQB_ERR_CUDA;
+  if (!rc && launch_fermi_init(c->d_fermi, c->d_result, c->stream) != cudaSuccess) rc = SQB_ERR_CUDA;
+  cudaGraphConditionalHandle h{};
+  if (!rc) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphNode_t wnode = nullptr;
+    cudaGraphNodeParams cp{};
+    if (cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &cg, &deps, &ndeps) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+      rc = SQB_ERR_CUDA;
+    } else {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      if (cudaGraphAddNode(&wnode, cg, deps, ndeps, &cp) != cudaSuccess ||
+          cudaStreamUpdateCaptureDependencies(c->stream, &wnode, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+        rc = SQB_ERR_CUDA;
+    }
+    if (!rc) {  // the loop body, captured on a second stream into the while node's graph
+      cudaStream_t bs = nullptr;
+      if (cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) != cudaSuccess) {
+        rc = SQB_ERR_CUDA;
+      } else {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        cudaGraph_t got = nullptr;
+        if (cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+          rc = SQB_ERR_CUDA;
+        if (!rc && launch_ne_constraint(fa, 0.0, deriv, bs) != cudaSuccess) rc = SQB_ERR_CUDA;
+        if (!rc && launch_fermi_step(c->d_fermi, c->d_result, h, bs) != cudaSuccess) rc = SQB_ERR_CUDA;
+        if (cudaStreamEndCapture(bs, &got) != cudaSuccess) rc = SQB_ERR_CUDA;
+        cudaStreamDestroy(bs);
+      }
+    }
+  }
+  if (!rc && launch_density_energy(fd, 0.0, c->stream) != cudaSuccess) rc = SQB_ERR_CUDA;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (!rc && e == cudaSuccess && cudaGraphInstantiate(&c->step_graph, g, 0) != cudaSuccess) c->step_graph = nullptr;
+  if (g) cudaGraphDestroy(g);
+  if (rc || e != cudaSuccess || !c->step_graph) {
+    cudaGetLastError();
+    c->step_graph = nullptr;
+    return rc ? rc : SQB_ERR_CUDA;
+  }
+  return SQB_OK;
+}
+
+static int run_step_graph(sqb_ctx *c, int scf_iter, double lambda_warm, double *lambda_f, double *rho,
+                          double *rho_pj, double *ci, double *chi, double *zee, double *ebs, double *eent) {
+  if (!c->step_graph) {
+    int rc0 = build_step_graph(c);
+    if (rc0) return rc0;
+  }
+  FermiDev st{};
+  st.alg = c->g.fermi_alg;
+  st.scf_iter = scf_iter;
+  st.lambda_warm = lambda_warm;
+  st.tol = c->g.fermi_tol;
+  st.h3 = pow(c->g.delta, 3);
+  st.ncharge = c->g.ncharge;
+  st.bet = c->g.bet;
+  CK(cudaMemcpyAsync(c->d_fermi, &st, sizeof(st), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  c->stats = sqb_stats{};
+  c->stats.window_points = (long long)c->n * c->n * c->n;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  CK(cudaGraphLaunch(c->step_graph, c->stream));
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaMemcpyAsync(&st, c->d_fermi, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  double r[2];
+  CK(cudaMemcpyAsync(r, c->d_result, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+  int stw = 0;
+  CK(cudaMemcpyAsync(&stw, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->stats.ms_lanczos_moments = elapsed(c);  // the whole step in graph mode
+  c->stats.node_kernel = SQB_KERNEL_SWEEP;
+  c->stats.kernel_launches = 1;
+  int rc = status_to_err(stw);
+  if (rc) return rc;
+  std::vector<int> its;
+  rc = lanczos_stats(c, its);
+  if (rc) return rc;
+  c->have_moments = true;
+  c->have_ci = true;
+  c->lmin_all = st.lmin_all;
+  c->lmax_all = st.lmax_all;
+  c->stats.fermi_iters = st.iters;
+  if (st.status == -1) return SQB_ERR_NOT_BRACKETED;
+  if (st.status == -2) return SQB_ERR_FERMI_MAXITER;
+  if (st.status != 1) return SQB_ERR_NONFINITE;
+  c->lambda_last = st.root;
+  *lambda_f = st.root;
+  if (st.dstat & 2) return SQB_ERR_NONFINITE;
+  const size_t N = c->nnode, K = c->g.npl + 1;
+  if (chi) CK(cudaMemcpy(chi, c->d_chi, N * sizeof(double), cudaMemcpyDeviceToHost));
+  if (zee) CK(cudaMemcpy(zee, c->d_zee, N * sizeof(double), cudaMemcpyDeviceToHost));
+  if (rho_pj) CK(cudaMemcpy(rho_pj, c->d_rho_pj, N * K * sizeof(double), cudaMemcpyDeviceToHost));
+  if (rho) CK(cudaMemcpy(rho, c->d_rho, N * sizeof(double), cudaMemcpyDeviceToHost));
+  if (ci) CK(cudaMemcpy(ci, c->d_ci, N * K * sizeof(double), cudaMemcpyDeviceToHost));
+  if (ebs) *ebs = r[0];
+  if (eent) *eent = r[1];
+  if (st.dstat & 1) return SQB_ERR_NEGATIVE_RHO;
+  return SQB_OK;
+}
+
 static int spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *rho, double *rho_pj, double *ci,
                                double *chi, double *zee, double *ebs, double *eent) {
+  const double tol_eff = std::max(c->g.lanczos_tol, c->mixed_lanczos_tol);
+  const bool defect = c->precision != SQB_FP64 && c->defect_budget > 0.0 && tol_eff > c->g.lanczos_tol;
+  if (c->use_graph == 2 && !c->allreduce && !defect && c->have_veff && c->have_atoms && c->have_proj) {
+    bool sw = false;
+    int rc0 = use_sweep(c, &sw);
+    if (rc0) return rc0;
+    if (sw) return run_step_graph(c, scf_iter, *lambda_f, lambda_f, rho, rho_pj, ci, chi, zee, ebs, eent);
+  }
   int rc = sqb_lanczos_moments(c, chi, zee, rho_pj, nullptr, nullptr, nullptr);
   if (rc) return rc;
   double lam = 0.0;
@@ -1376,7 +1531,7 @@ int sqb_set_node_kernel(sqb_ctx *c, int kernel) {
 }
 
 int sqb_set_graph(sqb_ctx *c, int on) {
-  if (!c || (on != 0 && on != 1)) return SQB_ERR_ARG;
+  if (!c || on < 0 || on > 2) return SQB_ERR_ARG;
   c->use_graph = on;
   drop_graph(c);
   return SQB_OK;

@@ -58,7 +58,8 @@ __device__ __forceinline__ double cheb_coeff(const double *dk, const double *cta
 
 // NeConstraint (sq.cpp:1183-1228) and, with deriv, NeConstraint_derv
 // (sq.cpp:1407-1449): per-block partial sums of 2 rho_pj . c.
-__global__ void __launch_bounds__(FTHREADS) ne_kernel(FermiArgs a, double lambda, int deriv, int fits) {
+__global__ void __launch_bounds__(FTHREADS) ne_kernel(FermiArgs a, double lambda_arg, int deriv, int fits) {
+  const double lambda = a.lam_dev ? *a.lam_dev : lambda_arg;
   extern __shared__ __align__(16) double fsm[];
   __shared__ double red[FW][2];
   const int K = a.npl + 1;
@@ -244,7 +245,8 @@ __global__ void sum_partials(const double *partial, int nblocks, int width, doub
 
 // Density and energies (sq.cpp:733-797): Ci (FermiDirac), rho = |2 mu.c|,
 // Ebs and Eent partial sums.
-__global__ void __launch_bounds__(FTHREADS) density_kernel(FermiArgs a, double lambda, int fits) {
+__global__ void __launch_bounds__(FTHREADS) density_kernel(FermiArgs a, double lambda_arg, int fits) {
+  const double lambda = a.lam_dev ? *a.lam_dev : lambda_arg;
   extern __shared__ __align__(16) double fsm[];
   __shared__ double red[FW][2];
   const int K = a.npl + 1;

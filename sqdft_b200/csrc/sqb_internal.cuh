@@ -206,8 +206,34 @@ struct FermiArgs {
   double *result;     // final sums
   double *rho, *ci;   // assembly outputs
   int *status;
+  const double *lam_dev;  // when set, the kernels read the Fermi level here (graph replay)
 };
 cudaError_t launch_ne_constraint(const FermiArgs &a, double lambda, int with_derivative, cudaStream_t s);
+
+// Fermi-level solve on the device (BrentsAlgorithm sq.cpp:1289-1404 or
+// NewtonRaphson sq.cpp:1459-1490, the host solvers' control flow and
+// arithmetic), one NeConstraint evaluation per step, for the whole SQ step
+// replayed as one CUDA graph with a conditional while node: fermi_init sets
+// the first trial level, each loop body runs NeConstraint at st->x and
+// fermi_step, which takes the sums, advances the solver and sets the loop
+// condition (0 once converged or failed).
+struct FermiDev {
+  int alg, scf_iter;          // 1 Brent, 2 Newton
+  double lambda_warm, tol, h3, ncharge, bet;
+  double a, b, cc, d, e, fa, fb, fc;  // Brent
+  int phase, iter;
+  double lold, lnew, err;     // Newton
+  int count;
+  double x;                   // the level the next NeConstraint evaluates
+  int steps;                  // evaluations so far (bounded)
+  int status;                 // 0 running, 1 converged, -1 not bracketed, -2 iteration limit, -3 non-finite
+  double root;
+  int iters;
+  int dstat;                  // the density assembly's status bits (1 negative rho, 2 non-finite)
+  double lmin_all, lmax_all;  // the spectral bracket of the step (min lmin, max lmax over nodes)
+};
+cudaError_t launch_fermi_init(FermiDev *st, const double *minmax, cudaStream_t s);
+cudaError_t launch_fermi_step(FermiDev *st, const double *sums, cudaGraphConditionalHandle h, cudaStream_t s);
 cudaError_t launch_density_energy(const FermiArgs &a, double lambda, cudaStream_t s);
 int fermi_blocks(int n_nodes);
 // Density-loss adjoint (sqb_density_loss_vjp): signs of the nodes' densities

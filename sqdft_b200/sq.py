@@ -206,8 +206,10 @@ class Context:
         """Kernel of the Lanczos bounds and moments: auto, plane-streaming or sweep."""
         _check(self.lib.sqb_set_node_kernel(self.ptr, int(kernel)), "sqb_set_node_kernel")
 
-    def set_graph(self, on: bool = True):
-        _check(self.lib.sqb_set_graph(self.ptr, int(bool(on))), "sqb_set_graph")
+    def set_graph(self, on=True):
+        """sqb_set_graph: False/0 plain launches, True/1 the node-kernel sequence from a graph,
+        2 the whole SQ step (Fermi solve included) as one graph."""
+        _check(self.lib.sqb_set_graph(self.ptr, int(on)), "sqb_set_graph")
 
     def autotune(self, sample: int = 0):
         """Pick the node kernel's layout by timing a node sample; returns the
