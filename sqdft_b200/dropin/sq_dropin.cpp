@@ -92,6 +92,12 @@ void ensure_ctx(DS_SQ *p) {
     if (rc) fail(rc, "sqb_set_mixed_lanczos");
   }
   if (p->nproc > 1) sqb_set_allreduce(g_ctx, mpi_reduce, nullptr);
+  // SQDFT_B200_GRAPH=2: every SCF iteration's SQ step replays one CUDA graph
+  // (node kernel, device-side Fermi solve, density); 1: the node kernel only
+  if (const char *gr = std::getenv("SQDFT_B200_GRAPH")) {
+    rc = sqb_set_graph(g_ctx, std::atoi(gr));
+    if (rc) fail(rc, "sqb_set_graph");
+  }
   std::atexit(destroy_ctx);
 }
 

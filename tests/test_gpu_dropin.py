@@ -42,7 +42,7 @@ def test_golden_run_matches_published_log():
     assert g["fermi_iters"] == pub["fermi_iters"]
 
 
-def run_program(tmp_path: Path, precision: str | None = None) -> dict:
+def run_program(tmp_path: Path, precision: str | None = None, graph: int = 0) -> dict:
     from sqdft_b200.configs.gen_configs import write_system
     from sqdft_b200.runlog import parse
 
@@ -54,6 +54,8 @@ def run_program(tmp_path: Path, precision: str | None = None) -> dict:
     env.pop("SQDFT_B200_EXPORT", None)
     if precision:
         env["SQDFT_B200_PRECISION"] = precision
+    if graph:
+        env["SQDFT_B200_GRAPH"] = str(graph)
     out = subprocess.run([str(PROGRAM), "-name", "al_ref"], cwd=run, env=env, capture_output=True, text=True,
                          timeout=900)
     (tmp_path / "sqdft_gpu.log").write_text(out.stdout + out.stderr)
@@ -90,3 +92,20 @@ def test_dropin_program_fast_forms(tmp_path, precision):
     assert len(got["scf"]) == len(g["scf"])
     assert de <= 1e-6
     assert df <= 1e-5
+
+
+@pytest.mark.gpu
+def test_dropin_program_scf_loop_on_step_graphs(tmp_path):
+    """The reference's SCF loop (Poisson, XC, Anderson mixing on the host) with
+    every SQ step replayed from one CUDA graph (SQDFT_B200_GRAPH=2: node kernel,
+    Fermi solve on the device, density): the same SCF history as the reference
+    run, to the tolerances of the plain drop-in run."""
+    g = json.loads(GOLDEN.read_text())
+    got = run_program(tmp_path, graph=2)
+    assert len(got["scf"]) == len(g["scf"])
+    for a, b in zip(got["scf"], g["scf"]):
+        assert abs(a["fermi"] - b["fermi"]) <= 1e-9, (a, b)
+        assert abs(a["etot"] - b["etot"]) <= 1e-9, (a, b)
+    assert got["fermi_iters"] == g["fermi_iters"]
+    assert abs(got["free_energy"] - g["free_energy"]) <= 1e-8
+    assert np.abs(np.array(got["forces"]) - np.array(g["forces"])).max() <= 1e-7
