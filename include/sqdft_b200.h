@@ -43,6 +43,8 @@ extern "C" {
 #define SQB_ERR_CAPACITY 10        /* more projector atoms in one window than supported */
 #define SQB_ERR_NONFINITE 11       /* NaN or Inf met in inputs or in a result */
 #define SQB_ERR_STATE 12           /* entry point called before its inputs were set */
+#define SQB_ERR_BOUNDS 13          /* a device index check failed (the bounds-check build,
+                                      libsqdft_b200_bc.so, only) */
 
 /* Precision of the recursion vectors (Chebyshev and Lanczos). */
 #define SQB_FP64 0        /* everything in FP64: parity path */

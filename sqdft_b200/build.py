@@ -1,9 +1,10 @@
 """Build the sqdft_b200 shared library for sm_100a with nvcc.
 
-    python -m sqdft_b200.build [--verbose-ptxas]
+    python -m sqdft_b200.build [--verbose-ptxas] [--bounds-check]
 
 Produces ``sqdft_b200/_build/libsqdft_b200.so`` in the source tree (it travels
-with the tree to the GPU host; it is not installed anywhere).
+with the tree to the GPU host; it is not installed anywhere), and with
+--bounds-check the index-checking variant ``libsqdft_b200_bc.so``.
 """
 from __future__ import annotations
 
@@ -35,16 +36,25 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def build(verbose_ptxas: bool = False, force: bool = False) -> Path:
-    BUILD.mkdir(parents=True, exist_ok=True)
+LIB_BC = BUILD / "libsqdft_b200_bc.so"
+
+
+def build(verbose_ptxas: bool = False, force: bool = False, bounds_check: bool = False) -> Path:
+    """The library; with bounds_check the index-checking variant
+    (-DSQB_BOUNDS_CHECK, libsqdft_b200_bc.so: a failed device index check
+    returns SQB_ERR_BOUNDS; load it with SQDFT_B200_LIB)."""
+    out_dir = BUILD / "bc" if bounds_check else BUILD
+    lib = LIB_BC if bounds_check else LIB
+    out_dir.mkdir(parents=True, exist_ok=True)
     deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [INCLUDE / "sqdft_b200.h"]
-    if LIB.exists() and not force and all(LIB.stat().st_mtime >= d.stat().st_mtime for d in deps):
-        return LIB
+    if lib.exists() and not force and all(lib.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return lib
     cmds, objs = [], []
     for src in SOURCES:
-        obj = BUILD / (Path(src).stem + ".o")
+        obj = out_dir / (Path(src).stem + ".o")
         cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-               *EXTRA.get(src, []), f"-I{INCLUDE}", "-c", str(CSRC / src), "-o", str(obj)]
+               *EXTRA.get(src, []), *(["-DSQB_BOUNDS_CHECK"] if bounds_check else []), f"-I{INCLUDE}", "-c",
+               str(CSRC / src), "-o", str(obj)]
         if verbose_ptxas:
             cmd.insert(-4, "-Xptxas=-v")
         cmds.append(cmd)
@@ -54,11 +64,12 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> Path:
         for r in pool.map(lambda c: subprocess.run(c, check=False), cmds):
             if r.returncode != 0:
                 raise subprocess.CalledProcessError(r.returncode, r.args)
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = lib.with_suffix(".so.tmp")
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
-    tmp.replace(LIB)
-    return LIB
+    tmp.replace(lib)
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose_ptxas="--verbose-ptxas" in sys.argv, force="--force" in sys.argv))
+    print(build(verbose_ptxas="--verbose-ptxas" in sys.argv, force="--force" in sys.argv,
+                bounds_check="--bounds-check" in sys.argv))

@@ -172,6 +172,7 @@ int status_to_err(int st) {
   // ST_LANCZOS_MAXITER is a warning: the reference prints and carries on with
   // the last Ritz values (sq.cpp:1073-1074); the nodes are counted in the stats.
   if (st & ST_WAIT_LIMIT) return SQB_ERR_CUDA;
+  if (st & ST_BOUNDS) return SQB_ERR_BOUNDS;
   return SQB_OK;
 }
 
@@ -689,6 +690,7 @@ const char *sqb_status_string(int st) {
     case SQB_ERR_CAPACITY: return "too many projector atoms in one truncation window";
     case SQB_ERR_NONFINITE: return "non-finite value";
     case SQB_ERR_STATE: return "inputs not set";
+    case SQB_ERR_BOUNDS: return "device index check failed (bounds-check build)";
     default: return "unknown status";
   }
 }

@@ -30,7 +30,20 @@ enum : int {
   ST_SPLINE_RANGE = 8,
   ST_FSLOTS = 16,
   ST_WAIT_LIMIT = 32,  // a bounded wait on an asynchronous copy ran out
+  ST_BOUNDS = 64,      // an index check of the bounds-check build failed
 };
+
+// Index checks of the bounds-check build (-DSQB_BOUNDS_CHECK; build.py makes
+// it as a second library beside the normal one): a failed check sets
+// ST_BOUNDS in the status word and redirects the access to element 0 (inside
+// every buffer), so the kernel runs on and the host returns SQB_ERR_BOUNDS.
+// In the normal build the checks compile to nothing.
+#ifdef SQB_BOUNDS_CHECK
+#define SQB_IDX(i, n, st) \
+  (((unsigned long long)(long long)(i) < (unsigned long long)(n)) ? (i) : (atomicOr((st), ST_BOUNDS), 0))
+#else
+#define SQB_IDX(i, n, st) (i)
+#endif
 
 // Replica atoms and projector tables as the node kernels read them.
 struct DevAtoms {

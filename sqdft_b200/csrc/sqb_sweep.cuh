@@ -173,14 +173,17 @@ __device__ __forceinline__ void reduce_instance(const SweepArgs &a, Shared &S, c
   const int n = a.n, n2 = n * n;
   const int x0 = S.e_x0[e], y0 = S.e_y0[e];
   const int bx = S.e_x1[e] - x0 + 1, by = S.e_y1[e] - y0 + 1, cnt = bx * by;
-  const double *f = fb + ((size_t)(k * PM + q) * n + S.e_z1[e]) * n2 + y0 * n + x0;
-  const double *fw = f + (size_t)KL * PM * n * n2;
+  const int base = ((k * PM + q) * n + S.e_z1[e]) * n2 + y0 * n + x0, set = KL * PM * n * n2;
+  const double *f = fb + base;
+  const double *fw = f + set;
+  (void)set;
   double s = 0.0, sw = 0.0;
 #pragma unroll 4
   for (int i = lane; i < cnt; i += 32) {
     const int yy = i / bx, xx = i - yy * bx;
-    s += f[yy * n + xx];
-    if constexpr (IND) sw += fw[yy * n + xx];
+    const int o = SQB_IDX(base + yy * n + xx, set, a.status) - base;
+    s += f[o];
+    if constexpr (IND) sw += fw[o];
   }
   s = warp_sum(s);
   if constexpr (IND) sw = warp_sum(sw);
@@ -231,6 +234,10 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   const double *veff = a.veff64;
   const unsigned long long *lid = a.lay_id;
   const double *lchi = a.lay_chi;
+  const int NW = n * n2;                     // window points (vector length)
+  int *const st = a.status;                  // (bounds-check build)
+  (void)NW;
+  (void)st;
 
   // zero the halo of both planes (the interior is written every plane)
   for (int i = tid; i < 2 * P2; i += NS) {
@@ -256,7 +263,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   T pf[RY], r1[RY], r2[RY];
   auto load_ops = [&](int j, int zz) {
     if (!ok[j] || zz >= n || io.konst) return;
-    const int g = zz * n2 + col[j];
+    const int g = SQB_IDX(zz * n2 + col[j], NW, st);
     pf[j] = io.vin[g];
     if constexpr (SK == SK_LZF) {
       r1[j] = io.p1[g];
@@ -271,7 +278,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
     else if (io.konst == 2) v = (T)(g == gc ? 1.0 : 0.0);
     else if constexpr (SK == SK_LZF) v = (T)(io.s1 * ((double)pf[j] - io.ca * (double)r1[j]) - io.cb * (double)r2[j]);
     else v = pf[j];
-    if constexpr (SK == SK_LZF) io.wout[g] = v;
+    if constexpr (SK == SK_LZF) io.wout[SQB_IDX(g, NW, st)] = v;
     return v;
   };
 
@@ -284,16 +291,17 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   double acd[RY][KL][PM];
   // IND: the input's partial of (layer k, row j) lives in accw[(k RY + j) NS + tid]
   auto load_ids = [&](int j, int zz) -> unsigned long long {
-    return (ok[j] && zz < n) ? __ldg(lid + xb[j] + zz * EP) : empty;
+    return (ok[j] && zz < n) ? __ldg(lid + SQB_IDX(xb[j] + zz * EP, EV, st)) : empty;
   };
   auto load_point = [&](int j, int zz) {
     if (!ok[j] || zz >= n) return;
-    const int X = xb[j] + zz * EP;
+    const int X = SQB_IDX(xb[j] + zz * EP, EV, st);
     if constexpr (STENCIL) ve[j] = __ldg(veff + X);
     if constexpr (CHEB) {
-      if (!io.first) q1[j] = io.p1_delta ? (T)(zz * n2 + col[j] == gc ? 1.0 : 0.0) : io.p1[zz * n2 + col[j]];
+      if (!io.first)
+        q1[j] = io.p1_delta ? (T)(zz * n2 + col[j] == gc ? 1.0 : 0.0) : io.p1[SQB_IDX(zz * n2 + col[j], NW, st)];
     }
-    if constexpr (SK == SK_FD) dq[j] = io.first ? 0.0 : io.dacc[zz * n2 + col[j]];
+    if constexpr (SK == SK_FD) dq[j] = io.first ? 0.0 : io.dacc[SQB_IDX(zz * n2 + col[j], NW, st)];
     if constexpr (CHR) {
 #pragma unroll
       for (int k = 0; k < KL; k++)
@@ -401,7 +409,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
           for (int k = 0; k < KL; k++) {
             const unsigned id = lay_of(idc[j], k);
 #pragma unroll
-            for (int q = 0; q < PM; q++) vnl += pcur[id + q] * chi_at(j, k, q, X);
+            for (int q = 0; q < PM; q++) vnl += pcur[SQB_IDX(id + q, a.n_gproj + PM, st)] * chi_at(j, k, q, X);
           }
           v[j] = (double)fut[j][C];
           hv[j] = -0.5 * temp[j] + ve[j] * v[j] + vnl;
@@ -410,7 +418,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
 #pragma unroll
       for (int j = 0; j < RY; j++) {
         if (!ok[j]) continue;
-        const int g = z * n2 + col[j];
+        const int g = SQB_IDX(z * n2 + col[j], NW, st);
         double o;
         if constexpr (SK == SK_ONES) {
           o = start_val(io.chk, g);
@@ -458,7 +466,7 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
             if (lay_of(chg, k) == 0u) continue;
             if (lay_of(idc[j], k) != dummy) {
 #pragma unroll
-              for (int q = 0; q < PM; q++) fb[((k * PM + q) * n + z) * n2 + col[j]] = acd[j][k][q];
+              for (int q = 0; q < PM; q++) fb[SQB_IDX(((k * PM + q) * n + z) * n2 + col[j], KL * PM * NW, st)] = acd[j][k][q];
               if constexpr (IND) fbw[(k * n + z) * n2 + col[j]] = accw[(k * RY + j) * NS + tid];
             }
 #pragma unroll
@@ -1039,7 +1047,7 @@ __device__ void node_forces(const SweepArgs &a, Shared &S, unsigned char *dyn, d
       double ax = 0.0, ay = 0.0, az = 0.0;
       for (int i = threadIdx.x; i < vol; i += blockDim.x) {
         const int x = x0 + i % bx, y = y0 + (i / bx) % by, z = z0 + i / (bx * by);
-        const int w = z * n2 + y * n + x;
+        const int w = SQB_IDX(z * n2 + y * n + x, n * n2, a.status);
         double gx = 0.0, gy = 0.0, gz = 0.0;
         for (int kk = 1; kk <= FDN; kk++) {
           const double xm = x - kk >= 0 ? D[w - kk] : 0.0, xp = x + kk < n ? D[w + kk] : 0.0;
@@ -1049,7 +1057,7 @@ __device__ void node_forces(const SweepArgs &a, Shared &S, unsigned char *dyn, d
           gy += (-ym + yp) * a.coeff_grad[kk];
           gz += (-zm + zp) * a.coeff_grad[kk];
         }
-        const double u = U[((S.gk + z) * a.ey + (S.gj + y)) * a.ex + S.gi + x];
+        const double u = U[SQB_IDX(((S.gk + z) * a.ey + (S.gj + y)) * a.ex + S.gi + x, EV, a.status)];
         ax += u * gx;
         ay += u * gy;
         az += u * gz;
