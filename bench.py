@@ -165,6 +165,55 @@ def run_sample(args):
                       "frac": abytes / kern / 1e9 / peak}), flush=True)
 
 
+def run_scf(args):
+    """The reference program's SCF loop on a configuration -- the drop-in
+    program (Poisson, exchange-correlation and Anderson mixing on the host,
+    the SQ step and forces through this library) -- for exactly
+    --scf-steps SCF iterations, each SQ step replayed from one CUDA graph
+    (--graph 2, the default here) or launched plainly (--graph 0).  One JSON
+    line: the device time of every SQ step from the library's metrics record,
+    the Brent iterations, the force pass and the program's wall time."""
+    import subprocess
+    import tempfile
+
+    from sqdft_b200.configs.gen_configs import write_system
+
+    prog = ROOT / "sqdft_b200" / "_build" / "dropin" / "sqdft_gpu"
+    pot = ROOT / "sqdft_b200" / "_data" / "pot"
+    n = args.scf_steps
+    with tempfile.TemporaryDirectory() as td:
+        run = write_system(args.config, Path(td))
+        inp = run / f"{args.config}.input"
+        text = inp.read_text().replace("scf_miniter 3", f"scf_miniter {n}").replace("scf_maxiter 40",
+                                                                                   f"scf_maxiter {n}")
+        inp.write_text(text)
+        for p in pot.glob("*.pot"):
+            (run / p.name).symlink_to(p)
+        metrics = Path(td) / "metrics.jsonl"
+        env = dict(os.environ, SQDFT_B200_GRAPH=str(args.graph), SQDFT_B200_METRICS=str(metrics))
+        env.pop("SQDFT_B200_EXPORT", None)
+        if args.precision in ("mixed", "lq"):
+            env["SQDFT_B200_PRECISION"] = "fp32" if args.precision == "mixed" else "lq"
+            env["SQDFT_B200_LANCZOS_TOL"] = str(args.mixed_lanczos_tol)
+        t0 = time.perf_counter()
+        out = subprocess.run([str(prog), "-name", args.config], cwd=run, env=env, capture_output=True, text=True,
+                             timeout=3600)
+        wall = time.perf_counter() - t0
+        recs = [json.loads(x) for x in metrics.read_text().splitlines()] if metrics.exists() else []
+    steps = [r for r in recs if r["call"] == "spectral_quadrature"]
+    forces = [r for r in recs if r["call"] == "forces_nonlocal"]
+    print(json.dumps({"mode": "scf", "config": args.config, "precision": args.precision, "graph": args.graph,
+                      "program_rc": out.returncode, "scf_iterations": len(steps),
+                      "sq_step_ms": [r["ms_lanczos_moments"] + r["ms_fermi"] + r["ms_density"] + r["ms_defect"]
+                                     for r in steps],
+                      "kernel_launches_per_step": [r["kernel_launches"] for r in steps],
+                      "fermi_iters": [r["fermi_iters"] for r in steps], "lambda_f": [r["lambda_f"] for r in steps],
+                      "forces_ms": [r["ms_forces"] for r in forces], "wall_s": wall,
+                      "nodes": steps[0]["nodes"] if steps else 0}), flush=True)
+    if out.returncode:
+        print(out.stdout[-2000:] + out.stderr[-2000:], file=sys.stderr)
+
+
 def run_forces(args):
     """ForcesNonLocal (forces.cpp:318-578) alone on a configuration after one
     SQ step of the given precision: W untimed and S timed force passes; one
@@ -543,9 +592,15 @@ def main():
                     help="window rows per sweep-kernel thread (0: the library's choice)")
     ap.add_argument("--forces-only", action="store_true",
                     help="one SQ step, then time ForcesNonLocal alone (needs --precision fp64|mixed)")
+    ap.add_argument("--scf-steps", type=int, default=0,
+                    help="run the drop-in program's SCF loop for this many iterations on --config")
+    ap.add_argument("--graph", type=int, default=2, choices=[0, 1, 2],
+                    help="with --scf-steps: graph mode of the SQ step (sqb_set_graph)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.scf_steps > 0:
+        run_scf(args)
     elif args.forces_only:
         run_forces(args)
     else:

@@ -1349,6 +1349,11 @@ int sqb_spectral_quadrature(sqb_ctx *c, int scf_iter, double *lambda_f, double *
 // several ranks go through the host) and without the defect check.
 static int build_step_graph(sqb_ctx *c) {
   if (!c->d_fermi) CK(cudaMalloc((void **)&c->d_fermi, sizeof(FermiDev)));
+  {  // allocate what the captured launches use (no allocation inside a capture)
+    size_t stride = 0;
+    const int rc0 = ensure_sweep_scratch(c, std::max(1, std::min(c->sms, c->nnode)), &stride);
+    if (rc0) return rc0;
+  }
   NodeArgs a;
   fill_node_args(c, a);
   a.mode = MODE_SQ;
