@@ -50,16 +50,30 @@ def test_node_lists_empty_duplicate_and_out_of_range(golden):
 def test_low_quadrature_orders_match_the_oracle(golden, npl):
     """The smallest quadrature orders (npl a multiple of 4 down to 4: a
     single doubling step, round(npl/4) = 1) on the Al cell: the sweep kernel's
-    bounds, moments, Fermi level and density equal the oracle's."""
+    bounds, moments, Fermi level and density equal the oracle's.  At npl 4
+    the expansion is too coarse for this cell and some node's density comes
+    out below -1e-6: the reference exits there ("Element of rho is negative",
+    sq.cpp:763-764), the oracle reports it, and the step returns
+    SQB_ERR_NEGATIVE_RHO after bounds, moments and Fermi level that still
+    equal the oracle's."""
     from oracle.pyoracle import Oracle
+    from sqdft_b200 import sq
 
     case, _ = golden("tiny")
     case = dataclasses.replace(case, npl=npl)
     ref = Oracle(case).spectral_quadrature()
     with _ctx(case) as ctx:
-        out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+        if ref["status"] != 0:
+            with pytest.raises(sq.SQBError) as err:
+                ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
+            assert err.value.code == 6  # SQB_ERR_NEGATIVE_RHO
+            out = ctx.lanczos_moments()
+            out["lambda_f"], _ = ctx.fermi_level(case.scf_iter, case.lambda_f)
+        else:
+            out = ctx.spectral_quadrature(case.scf_iter, case.lambda_f)
     assert np.abs(out["chi"] - ref["chi"]).max() <= 1e-10
     assert np.abs(out["zee"] - ref["zee"]).max() <= 1e-10
     assert np.abs(out["rho_pj"] - ref["rho_pj"]).max() <= 1e-10 * np.abs(ref["rho_pj"]).max()
     assert abs(out["lambda_f"] - ref["lambda_f"]) <= 1e-10
-    assert np.abs(out["rho"].ravel() - np.asarray(ref["rho"]).ravel()).max() <= 1e-10
+    if ref["status"] == 0:
+        assert np.abs(out["rho"].ravel() - np.asarray(ref["rho"]).ravel()).max() <= 1e-10
