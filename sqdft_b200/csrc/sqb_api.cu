@@ -188,11 +188,14 @@ int ensure_tmp(sqb_ctx *c, size_t bytes) {
 // Columns per thread of the node kernel: 0 lets the launcher pick its layout.
 int choose_cols(const sqb_ctx *c) { return c->cols; }
 
+void drop_graph(sqb_ctx *c);
+
 int ensure_scratch(sqb_ctx *c, int grid) {
   const size_t nw = (size_t)c->n * c->n * c->n;
   c->scratch_stride = ((4 * nw * sizeof(double)) + 255) & ~size_t(255);
   const size_t need = c->scratch_stride * (size_t)grid;
   if (c->scratch_bytes < need) {
+    drop_graph(c);  // captured launches hold the old buffer's address
     if (c->d_scratch) cudaFree(c->d_scratch);
     c->d_scratch = nullptr;
     CK(cudaMalloc((void **)&c->d_scratch, need));
@@ -383,6 +386,7 @@ int use_sweep(sqb_ctx *c, bool *yes) {
 int ensure_sweep_scratch(sqb_ctx *c, int grid, size_t *stride) {
   *stride = sweep_scratch_bytes(c->n, c->lay_pmax);
   if (c->scratch_bytes < *stride * (size_t)grid) {
+    drop_graph(c);  // captured launches hold the old buffer's address
     if (c->d_scratch) cudaFree(c->d_scratch);
     c->d_scratch = nullptr;
     c->scratch_bytes = 0;
@@ -888,6 +892,7 @@ int sqb_set_atoms(sqb_ctx *c, int n_typ, const sqb_species *types, int n_rep, co
   }
   std::vector<int> nn((size_t)4 * std::max(n_rep, 1));
   c->lay_state = 0;  // the layered fields follow the projector tables
+  drop_graph(c);    // (their buffers are rebuilt; captured launches hold the old addresses)
   std::vector<long long> off(std::max(n_rep, 1)), off_ref(std::max(n_rep, 1));
   long long total = 0, total_pad = 0;
   for (int r = 0; r < n_rep; r++) {
@@ -1004,6 +1009,7 @@ int sqb_nonlocal_projectors(sqb_ctx *c, double *udvtm_out) {
   c->have_proj = true;
   c->have_moments = false;
   c->lay_state = 0;
+  drop_graph(c);  // the layered fields are rebuilt from the new tables
   return SQB_OK;
 }
 
@@ -1023,6 +1029,7 @@ int sqb_set_projectors(sqb_ctx *c, const double *udvtm) {
   c->have_proj = true;
   c->have_moments = false;
   c->lay_state = 0;
+  drop_graph(c);  // the layered fields are rebuilt from the new tables
   return SQB_OK;
 }
 

@@ -427,3 +427,24 @@ def test_whole_step_graph_matches_host_driven_step(golden, name, fermi_alg):
         assert p["Ebs"] == g["Ebs"] and p["Eent"] == g["Eent"]
         for k in keys:
             assert np.array_equal(p[k], g[k]), k
+
+
+def test_whole_step_graph_follows_new_projector_tables(golden):
+    """New projector tables between replays of the whole-step graph: the
+    layered projector fields are rebuilt in new buffers, so the captured graph
+    is dropped and recaptured, and the step equals a fresh context's with the
+    new tables bit for bit."""
+    case, _ = golden("lihs")
+    scaled = case.udvtm * 0.9
+    with _ctx(case) as ctx:
+        ctx.set_graph(2)
+        ctx.spectral_quadrature(1, case.lambda_f)
+        ctx.spectral_quadrature(2, case.lambda_f)  # replay
+        ctx.set_projectors(scaled)
+        moved = ctx.spectral_quadrature(2, case.lambda_f)
+    with _ctx(case) as ref:
+        ref.set_projectors(scaled)
+        want = ref.spectral_quadrature(2, case.lambda_f)
+    assert moved["lambda_f"] == want["lambda_f"]
+    for k in ("chi", "zee", "rho_pj", "rho"):
+        assert np.array_equal(moved[k], want[k]), k
