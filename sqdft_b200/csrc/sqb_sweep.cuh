@@ -53,6 +53,9 @@ constexpr int RY_DEFAULT = 2;  // window rows per thread (3 for fields with thre
 enum : int { SK_ONES = 0, SK_LZF = 1, SK_CH = 2, SK_FD = 3 };
 
 struct Shared {
+  unsigned long long pbar;  // plane barrier of the sweeps (mbarrier, one arrival per thread and plane)
+  unsigned pbar_phase;      // its phases completed so far
+  int wabort;               // a plane wait ran out of time: later waits are skipped
   int node, qidx, gi, gj, gk;
   int n_ent, n_pi;
   int stop, count;
@@ -86,12 +89,16 @@ struct Shared {
 };
 
 __host__ __device__ constexpr int plane_pitch(int n) { return n + 2 * FDN; }
-// two halo'd planes, plus ry - 1 rows of slack: the shared y-arm loads of a
-// row group whose last rows lie beyond the window read up to ry - 1 rows past
-// the plane (into values that are not used)
+// Halo'd planes of the stencil input: plane z lives in buffer z mod NPLANE.
+// Three buffers let a thread write plane z + 1 before it works on plane z
+// while the slowest thread may still read plane z - 1 (see sweep).
+constexpr int NPLANE = 3;
+// NPLANE halo'd planes, plus ry - 1 rows of slack: the shared y-arm loads of
+// a row group whose last rows lie beyond the window read up to ry - 1 rows
+// past the plane (into values that are not used)
 __host__ __device__ inline size_t planes_bytes(int n, int ry) {
   const int P = plane_pitch(n);
-  return ((size_t)(2 * P * P + (ry - 1) * P + 8) * sizeof(double) + 127) & ~size_t(127);
+  return ((size_t)(NPLANE * P * P + (ry - 1) * P + 8) * sizeof(double) + 127) & ~size_t(127);
 }
 // Lanczos sweeps of the one-projector fields also accumulate the dot products
 // of their input (the exact chi^T W_m, see lanczos), flushed into a second
@@ -128,6 +135,61 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Barrier of the block's threads inside a sweep (named barrier 1).
 __device__ __forceinline__ void bar_sweep(int nthreads) {
   asm volatile("bar.sync 1, %0;\n" ::"r"(nthreads) : "memory");
+}
+
+// The plane barrier: an mbarrier in shared memory that every thread of the
+// block arrives on once per plane (release: its plane writes are visible to
+// the threads whose wait on that phase returns, acquire).
+__device__ __forceinline__ unsigned pbar_addr(const unsigned long long *bar) {
+  return (unsigned)__cvta_generic_to_shared(bar);
+}
+__device__ __forceinline__ void pbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(pbar_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void pbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(pbar_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool pbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(pbar_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Every thread of the block arrives once per plane, so a phase completes in
+// microseconds; a wait that outlasts PBAR_WAIT_NS means a thread stopped
+// arriving: the wait sets the status bit and the block's abort flag, after
+// which no plane wait blocks (the step's results are then void and the call
+// returns an error).
+constexpr unsigned long long PBAR_WAIT_NS = 2000000000ull;
+__device__ __forceinline__ void pbar_wait(Shared &S, int *status, unsigned phase) {
+  if (*(volatile int *)&S.wabort) return;
+  const unsigned parity = phase & 1u;
+  if (pbar_try_wait(&S.pbar, parity)) return;
+  const unsigned long long t0 = gtimer_ns();
+  while (!pbar_try_wait(&S.pbar, parity)) {
+    if (gtimer_ns() - t0 > PBAR_WAIT_NS) {
+      *(volatile int *)&S.wabort = 1;
+      atomicOr(status, ST_WAIT_LIMIT);
+      return;
+    }
+  }
+}
+// Set up the plane barrier at the start of a kernel (before any sweep).
+__device__ __forceinline__ void pbar_setup(Shared &S) {
+  if (threadIdx.x == 0) {
+    pbar_init(&S.pbar, blockDim.x);
+    S.pbar_phase = 0u;
+    S.wabort = 0;
+  }
+  __syncthreads();
 }
 
 template <typename T>
@@ -239,8 +301,8 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   (void)NW;
   (void)st;
 
-  // zero the halo of both planes (the interior is written every plane)
-  for (int i = tid; i < 2 * P2; i += NS) {
+  // zero the halo of the planes (the interior is written every plane)
+  for (int i = tid; i < NPLANE * P2; i += NS) {
     const int r = (i % P2) / P, c = i % P;
     if (r < FDN || r >= n + FDN || c < FDN || c >= n + FDN) sm[i] = T(0);
   }
@@ -348,14 +410,33 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
   const double rcb = CHEB ? 1.0 / io.cb : 0.0;
   const double cdh = io.cd / a.h3, ceh = io.ce / a.h3;
 
-  for (int z = 0; z < n; z++) {
-    T *smz = sm + (z & 1) * P2;
-    if constexpr (STENCIL) {
+  // Planes through the shared buffers with a split barrier: in step z a
+  // thread first writes its centre values of plane z + 1 (buffer (z+1) mod 3)
+  // and arrives, then works on plane z, and only then waits until every
+  // thread has written plane z + 1.  A thread in step z has seen every thread
+  // arrive in step z - 1, so the slowest is at worst in step z - 1, reading
+  // buffer (z-1) mod 3: one buffer apart from the one written.  Warps drift
+  // by up to a plane instead of meeting at every plane.
+  const int sofs = (yb + FDN) * P + x + FDN;  // the thread's first row in a plane buffer
+  if constexpr (STENCIL) {
 #pragma unroll
-      for (int j = 0; j < RY; j++)
-        if (ok[j]) smz[(y[j] + FDN) * P + x + FDN] = fut[j][C];
+    for (int j = 0; j < RY; j++)
+      if (ok[j]) sm[sofs + j * P] = fut[j][C];
+  }
+  bar_sweep(NS);  // halo and plane 0 written; the previous sweep's phases are counted
+  const unsigned ph0 = S.pbar_phase;
+  int bz = 0;  // buffer of plane z
+  for (int z = 0; z < n; z++) {
+    T *smz = sm + bz * P2;
+    const int bn = bz == NPLANE - 1 ? 0 : bz + 1;
+    if constexpr (STENCIL) {
+      if (z + 1 < n) {
+#pragma unroll
+        for (int j = 0; j < RY; j++)
+          if (ok[j]) sm[bn * P2 + sofs + j * P] = fut[j][C + 1];
+        pbar_arrive(&S.pbar);
+      }
     }
-    bar_sweep(NS);
     if (tv) {
       double hv[RY], v[RY];
       if constexpr (STENCIL) {
@@ -490,6 +571,15 @@ __device__ __forceinline__ void sweep(const SweepArgs &a, Shared &S, unsigned ch
         load_ops(j, z + FDN + 2);
       }
     }
+    if constexpr (STENCIL) {
+      if (z + 1 < n) pbar_wait(S, a.status, ph0 + (unsigned)z);
+    }
+    bz = bn;
+  }
+  if constexpr (STENCIL) {
+    // every thread read ph0 before its first arrival, and thread 0 passed
+    // every wait of this sweep
+    if (tid == 0) S.pbar_phase = ph0 + (unsigned)(n - 1);
   }
   // balls that end at the window's last plane: every layer's open partial (a
   // layer with no ball there writes a zero no reduction reads); then every
@@ -1095,6 +1185,7 @@ __global__ void __launch_bounds__(MAXT, 1) sweep_force_kernel(SweepArgs a) {
   double *pcur =
       reinterpret_cast<double *>(dyn + planes_bytes(a.n, RY) + ring_bytes(a.nsweep, PM, RY) + accw_bytes(a.nsweep, PM, RY));
   for (int i = threadIdx.x; i < a.n_gproj + PM; i += blockDim.x) pcur[i] = 0.0;  // [n_gproj..]: the empty id
+  pbar_setup(S);
   for (;;) {
     if (threadIdx.x == 0) {
       const int q = atomicAdd(a.counter, 1);
@@ -1159,6 +1250,7 @@ __global__ void __launch_bounds__(MAXT, 1) sweep_kernel(SweepArgs a) {
   double *pcur =
       reinterpret_cast<double *>(dyn + planes_bytes(a.n, RY) + ring_bytes(a.nsweep, PM, RY) + accw_bytes(a.nsweep, PM, RY));
   for (int i = threadIdx.x; i < a.n_gproj + PM; i += blockDim.x) pcur[i] = 0.0;  // [n_gproj..]: the empty id
+  pbar_setup(S);
   for (;;) {
     if (threadIdx.x == 0) {
       const int q = atomicAdd(a.counter, 1);
