@@ -31,6 +31,11 @@ class _Problem(C.Structure):
     ]
 
 
+class _Local(C.Structure):
+    _fields_ = [("n_typ", C.c_int), ("typ_size", _ip), ("typ_tab", C.POINTER(_dp)), ("Z", _dp), ("n_rep", C.c_int),
+                ("rep_type", _ip), ("rep_atom", _ip), ("rep_xyz", _dp), ("rep_box", _ip), ("rc_tilda", C.c_double)]
+
+
 class _Psd(C.Structure):
     _fields_ = [("size", C.c_int), ("lmax", C.c_int), ("lloc", C.c_int), ("nlocc", C.c_int), ("tables", _dp)]
 
@@ -53,6 +58,9 @@ def _lib():
     lib.sqo_fermi_level.argtypes = [P, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _ip]
     lib.sqo_density_energy.argtypes = [P, _dp, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp]
     lib.sqo_forces_nonlocal.argtypes = [P, _ip, C.c_int, _dp, _dp, _dp, _dp]
+    LP = C.POINTER(_Local)
+    lib.sqo_charge_density.argtypes = [P, LP, _dp, _dp, _dp, _dp, _dp]
+    lib.sqo_forces_local.argtypes = [P, LP, _dp, _dp, _dp, _dp, _dp, _dp]
     return lib
 
 
@@ -192,3 +200,60 @@ class Oracle:
         out["lambda_f"] = lam
         out["fermi_iters"] = it
         return out
+
+
+class LocalOracle:
+    """ChargeDensity (initialize.cpp:470-784) and ForcesLocal (forces.cpp:20-315)
+    of the C restatement on one block.  ``loc`` is a
+    :class:`sqdft_b200.pseudocharge.LocalAtoms`; the grid comes from ``grid``,
+    an object with ``np_``, ``pnode_s``, ``fdn``, ``delta``, ``coeff_lap``,
+    ``coeff_grad`` and ``n_atm``."""
+
+    def __init__(self, grid, loc):
+        self.lib = _lib()
+        self.grid, self.loc = grid, loc
+        self.coeff_lap = np.ascontiguousarray(grid.coeff_lap, np.float64)
+        self.coeff_grad = np.ascontiguousarray(grid.coeff_grad, np.float64)
+        p = _Problem()
+        p.np[:] = list(grid.np_)
+        p.pnode_s[:] = list(grid.pnode_s)
+        p.fdn, p.delta, p.n_atm = grid.fdn, grid.delta, grid.n_atm
+        p.coeff_lap, p.coeff_grad = _d(self.coeff_lap), _d(self.coeff_grad)
+        self.p = p
+        self.tabs = [np.ascontiguousarray(t, np.float64) for t in loc.tables]
+        self.sizes = np.array([t.shape[1] for t in self.tabs], np.int32)
+        self.tab_ptrs = (_dp * len(self.tabs))(*[_d(t) for t in self.tabs])
+        self.Z = np.ascontiguousarray(loc.Z, np.float64)
+        self.rep_type = np.ascontiguousarray(loc.rep_type, np.int32)
+        self.rep_atom = np.ascontiguousarray(loc.rep_atom, np.int32)
+        self.rep_xyz = np.ascontiguousarray(loc.rep_xyz, np.float64)
+        self.rep_box = np.ascontiguousarray(loc.rep_box, np.int32)
+        L = _Local()
+        L.n_typ, L.typ_size, L.typ_tab, L.Z = len(self.tabs), _i(self.sizes), self.tab_ptrs, _d(self.Z)
+        L.n_rep = len(self.rep_type)
+        L.rep_type, L.rep_atom, L.rep_xyz, L.rep_box = (_i(self.rep_type), _i(self.rep_atom), _d(self.rep_xyz),
+                                                        _i(self.rep_box))
+        L.rc_tilda = loc.rc_tilda
+        self.L = L
+
+    def _shape(self):
+        return tuple(self.grid.np_[::-1])
+
+    def charge_density(self) -> dict:
+        sh = self._shape()
+        b, bt, vc, ra = (np.zeros(sh) for _ in range(4))
+        scal = np.zeros(7)
+        rc = self.lib.sqo_charge_density(C.byref(self.p), C.byref(self.L), _d(b), _d(bt), _d(vc), _d(ra), _d(scal))
+        if rc != 0:
+            raise RuntimeError("spline out of range in ChargeDensity")
+        return dict(b=b, b_tilda=bt, vc=vc, rho_at=ra, Eself=scal[0], Ncharge=scal[1], Nelectron_at=scal[2],
+                    Ncharge_tilda=scal[3], Eself_tilda=scal[4], Vcon=scal[5], Ecorr=scal[6])
+
+    def forces_local(self, phi, vc, b, b_tilda):
+        n = self.grid.n_atm
+        floc, fcorr = np.zeros((n, 3)), np.zeros((n, 3))
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (phi, vc, b, b_tilda)]
+        rc = self.lib.sqo_forces_local(C.byref(self.p), C.byref(self.L), *[_d(a) for a in arrs], _d(floc), _d(fcorr))
+        if rc != 0:
+            raise RuntimeError("spline out of range in ForcesLocal")
+        return floc, fcorr

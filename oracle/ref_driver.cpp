@@ -14,6 +14,10 @@
 //   --no-forces      skip ForcesNonLocal
 //   --hv K           also apply HsubTimesVec to K seeded vectors at K nodes
 //   --nodes-only     stop after the SQ set-up (export the inputs only)
+//   --local          also write <out_prefix>_local.sqc: the pseudocharge
+//                    replicas and radial tables, ChargeDensity's outputs
+//                    (initialize.cpp:470-784) as the call leaves them, and
+//                    ForcesLocal (forces.cpp:20-315) with the fields it read
 //   --sample K       CPU baseline: time the reference's per-node work
 //                    (LanczosAlgorithm, sq.cpp:965, and the moment loop of
 //                    sq.cpp:564-655 over HsubTimesVec) on K nodes spread over
@@ -118,7 +122,7 @@ int main(int argc, char **argv) {
   }
   std::string run_dir = argv[1], stem = argv[2], out = argv[3];
   std::string veff_file;
-  int scf_iter = 1, hv_count = 0, do_forces = 1, nodes_only = 0, sample = 0, threads = 1;
+  int scf_iter = 1, hv_count = 0, do_forces = 1, nodes_only = 0, sample = 0, threads = 1, do_local = 0;
   double lambda_warm = 0.0;
   int have_lambda = 0;
   for (int a = 4; a < argc; a++) {
@@ -128,6 +132,7 @@ int main(int argc, char **argv) {
     else if (!std::strcmp(argv[a], "--no-forces")) do_forces = 0;
     else if (!std::strcmp(argv[a], "--hv") && a + 1 < argc) hv_count = std::atoi(argv[++a]);
     else if (!std::strcmp(argv[a], "--nodes-only")) nodes_only = 1;
+    else if (!std::strcmp(argv[a], "--local")) do_local = 1;
     else if (!std::strcmp(argv[a], "--sample") && a + 1 < argc) sample = std::atoi(argv[++a]);
     else if (!std::strcmp(argv[a], "--threads") && a + 1 < argc) threads = std::atoi(argv[++a]);
     else { std::fprintf(stderr, "unknown option %s\n", argv[a]); return 2; }
@@ -159,10 +164,20 @@ int main(int argc, char **argv) {
   SQ.MDstepCount = 1;
 
   Replica_atoms(&SQ);
+  // ChargeDensity accumulates rho_at; the allocation zeroed it
+  double t0 = MPI_Wtime();
   ChargeDensity(&SQ);
+  const double t_cd = MPI_Wtime() - t0;
+  std::vector<double> cd_b, cd_bt, cd_vc, cd_rho_at;
+  if (do_local) {
+    cd_b = sqb::block_field(SQ.b, SQ.np_z, SQ.np_y, SQ.np_x, 0);
+    cd_bt = sqb::block_field(SQ.b_tilda, SQ.np_z, SQ.np_y, SQ.np_x, 0);
+    cd_vc = sqb::block_field(SQ.Vc, SQ.np_z, SQ.np_y, SQ.np_x, 0);
+    cd_rho_at = sqb::block_field(SQ.rho_at, SQ.np_z, SQ.np_y, SQ.np_x, 0);
+  }
   if (SQ.Correction == 2) OverlapCorrection(&SQ);
   Replica_atoms_Rcut(&SQ);
-  double t0 = MPI_Wtime();
+  t0 = MPI_Wtime();
   NonlocalProjectors(&SQ);
   double t_proj = MPI_Wtime() - t0;
   PoissonSolver_AAJ(&SQ);
@@ -312,6 +327,37 @@ int main(int argc, char **argv) {
     w.f64s("t_forces", t_f);
   }
   w.close();
+
+  if (do_local) {
+    sqb::CaseWriter wl(out + "_local.sqc");
+    // the pseudocharge inputs and the fields ForcesLocal reads (phi, Vc, b, b_tilda)
+    sqb::export_local(&SQ, wl);
+    const int nz = SQ.np_z, ny = SQ.np_y, nx = SQ.np_x;
+    wl.f64("cd_b", cd_b.data(), {nz, ny, nx});
+    wl.f64("cd_b_tilda", cd_bt.data(), {nz, ny, nx});
+    wl.f64("cd_vc", cd_vc.data(), {nz, ny, nx});
+    wl.f64("cd_rho_at", cd_rho_at.data(), {nz, ny, nx});
+    wl.f64s("cd_Eself", SQ.Eself);
+    wl.f64s("cd_Ncharge", SQ.Ncharge);
+    wl.f64s("cd_Ecorr", SQ.Ecorr);
+    wl.f64s("t_charge_density", t_cd);
+    t0 = MPI_Wtime();
+    ForcesLocal(&SQ);
+    const double t_fl = MPI_Wtime() - t0;
+    std::vector<double> fl((size_t)SQ.n_atm * 3), fc((size_t)SQ.n_atm * 3);
+    for (int a = 0; a < SQ.n_atm; a++) {
+      fl[3 * a] = SQ.flocx[a];
+      fl[3 * a + 1] = SQ.flocy[a];
+      fl[3 * a + 2] = SQ.flocz[a];
+      fc[3 * a] = SQ.fcorrx[a];
+      fc[3 * a + 1] = SQ.fcorry[a];
+      fc[3 * a + 2] = SQ.fcorrz[a];
+    }
+    wl.f64("fl_floc", fl.data(), {SQ.n_atm, 3});
+    wl.f64("fl_fcorr", fc.data(), {SQ.n_atm, 3});
+    wl.f64s("t_forces_local", t_fl);
+    wl.close();
+  }
   std::printf("sqref_driver: wrote %s_in.sqc and %s_out.sqc (SQ %.3f s)\n", out.c_str(), out.c_str(), t_sq);
   return 0;
 }

@@ -756,3 +756,198 @@ int sqo_projectors(const sqo_problem *p, const sqo_psd *psd, double *udvtm) {
   }
   return 0;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Pseudocharge density and local forces                                  */
+/* ---------------------------------------------------------------------- */
+
+/* VlocJ and VlocJ_tilda of one replica at a grid node (initialize.cpp:565-597,
+ * forces.cpp:116-143): the spline of r Vloc divided by r (the first table
+ * point's ratio at the nucleus) and the smooth reference potential of
+ * radius rc_tilda.  *rad receives r. */
+static int vloc_at(const sqo_local *L, int t, const double *c, double h, int gi, int gj, int gk, double *v,
+                   double *vt, double *rad) {
+  const double *G = L->typ_tab[t], *rV = G + L->typ_size[t], *DV = G + 2 * (size_t)L->typ_size[t];
+  const double dx = gi * h - c[0], dy = gj * h - c[1], dz = gk * h - c[2];
+  const double r = sqrt(dx * dx + dy * dy + dz * dz);
+  double s;
+  if (spline_at(G, rV, DV, L->typ_size[t], r, &s)) return -1;
+  *v = fabs(r - 0.0) < TEMP_TOL ? rV[1] / G[1] : s / r;
+  const double rc = L->rc_tilda, Z = L->Z[t];
+  if (r < rc)
+    *vt = -Z * (9 * pow(r, 7) - 30 * rc * pow(r, 6) + 28 * rc * rc * pow(r, 5) - 14 * pow(rc, 5) * pow(r, 2) +
+                12 * pow(rc, 7)) /
+          (5 * pow(rc, 8));
+  else
+    *vt = -Z / r;
+  *rad = r;
+  return 0;
+}
+
+/* -(1/4 pi) Lap_h of a box field at box index (i, j, k) (the stencil of
+ * initialize.cpp:604-614 and forces.cpp:154-170). */
+static double neg_lap(const sqo_problem *p, const double *f, int nx, int ny, int i, int j, int k) {
+  const double *cl = p->coeff_lap;
+#define F(ii, jj, kk) f[((size_t)(kk) * ny + (jj)) * nx + (ii)]
+  double s = F(i, j, k) * 3 * cl[0] * (-1 / (4 * M_PI));
+  for (int a = 1; a <= p->fdn; a++)
+    s += (F(i - a, j, k) + F(i + a, j, k) + F(i, j - a, k) + F(i, j + a, k) + F(i, j, k - a) + F(i, j, k + a)) * cl[a] *
+         (-1 / (4 * M_PI));
+#undef F
+  return s;
+}
+
+int sqo_charge_density(const sqo_problem *p, const sqo_local *L, double *b, double *b_tilda, double *vc,
+                       double *rho_at, double *scal) {
+  const int NX = p->np[0], NY = p->np[1], NZ = p->np[2], fdn = p->fdn;
+  const size_t N = (size_t)NX * NY * NZ;
+  const double h = p->delta;
+  memset(b, 0, N * sizeof(double));
+  memset(b_tilda, 0, N * sizeof(double));
+  memset(vc, 0, N * sizeof(double));
+  memset(rho_at, 0, N * sizeof(double));
+  double Eself = 0.0, Ncharge = 0.0, Nel = 0.0, Eself_t = 0.0, Ncharge_t = 0.0, Vcon = 0.0;
+  for (int r = 0; r < L->n_rep; r++) {
+    const int t = L->rep_type[r];
+    const int *bx = L->rep_box + 6 * r;
+    const double *c = L->rep_xyz + 3 * r;
+    const double *G = L->typ_tab[t], *U = G + 3 * (size_t)L->typ_size[t], *DU = G + 4 * (size_t)L->typ_size[t];
+    const int nx = bx[1] - bx[0] + 1 + 2 * fdn, ny = bx[3] - bx[2] + 1 + 2 * fdn, nz = bx[5] - bx[4] + 1 + 2 * fdn;
+    const int i0 = bx[0] - fdn, j0 = bx[2] - fdn, k0 = bx[4] - fdn;
+    double *V = malloc(sizeof(double) * nx * ny * nz), *Vt = malloc(sizeof(double) * nx * ny * nz);
+    /* initialize.cpp:565-597 */
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          const size_t q = ((size_t)k * ny + j) * nx + i;
+          double rad;
+          if (vloc_at(L, t, c, h, i0 + i, j0 + j, k0 + k, &V[q], &Vt[q], &rad)) {
+            free(V);
+            free(Vt);
+            return -1;
+          }
+          if (i >= fdn && i < nx - fdn && j >= fdn && j < ny - fdn && k >= fdn && k < nz - fdn) {
+            double rho_temp;
+            if (spline_at(G, U, DU, L->typ_size[t], rad, &rho_temp)) {
+              free(V);
+              free(Vt);
+              return -1;
+            }
+            rho_at[((size_t)(k + k0 - p->pnode_s[2]) * NY + (j + j0 - p->pnode_s[1])) * NX + (i + i0 - p->pnode_s[0])] +=
+                rho_temp;
+            Nel += rho_temp * h * h * h;
+          }
+        }
+    /* initialize.cpp:600-628 */
+    for (int k = bx[4]; k <= bx[5]; k++)
+      for (int j = bx[2]; j <= bx[3]; j++)
+        for (int i = bx[0]; i <= bx[1]; i++) {
+          const int ii = i - i0, jj = j - j0, kk = k - k0;
+          const size_t q = ((size_t)kk * ny + jj) * nx + ii;
+          const double bt = neg_lap(p, V, nx, ny, ii, jj, kk), btt = neg_lap(p, Vt, nx, ny, ii, jj, kk);
+          const size_t g = ((size_t)(k - p->pnode_s[2]) * NY + (j - p->pnode_s[1])) * NX + (i - p->pnode_s[0]);
+          b[g] += bt;
+          Eself += 0.5 * bt * V[q] * h * h * h;
+          Ncharge += bt * h * h * h;
+          b_tilda[g] += btt;
+          Eself_t += 0.5 * btt * Vt[q] * h * h * h;
+          Ncharge_t += btt * h * h * h;
+          vc[g] += Vt[q] - V[q];
+        }
+    /* initialize.cpp:631-635: Vcon at the main domain's first node */
+    if (bx[0] <= 0 && bx[1] >= 0 && bx[2] <= 0 && bx[3] >= 0 && bx[4] <= 0 && bx[5] >= 0) {
+      const size_t q = ((size_t)(0 - k0) * ny + (0 - j0)) * nx + (0 - i0);
+      Vcon += Vt[q] - V[q];
+    }
+    free(V);
+    free(Vt);
+  }
+  /* initialize.cpp:729-780 (one rank: the reductions are the local sums,
+   * V000 and Vcon the block's own) */
+  const double s = fabs(Ncharge / Ncharge_t), V000 = vc[0], h3 = pow(h, 3);
+  double Ecorr = 0.0;
+  for (size_t g = 0; g < N; g++) b_tilda[g] = s * b_tilda[g];
+  for (size_t g = 0; g < N; g++) {
+    vc[g] += -V000 + Vcon;
+    Ecorr += 0.5 * (b_tilda[g] + b[g]) * vc[g] * h3;
+  }
+  scal[0] = Eself;
+  scal[1] = Ncharge;
+  scal[2] = Nel;
+  scal[3] = Ncharge_t;
+  scal[4] = Eself_t;
+  scal[5] = Vcon;
+  scal[6] = Ecorr + Eself - Eself_t;
+  return 0;
+}
+
+int sqo_forces_local(const sqo_problem *p, const sqo_local *L, const double *phi, const double *vc, const double *b,
+                     const double *b_tilda, double *floc, double *fcorr) {
+  const int NX = p->np[0], NY = p->np[1], fdn = p->fdn;
+  const int PX = NX + 2 * fdn, PY = NY + 2 * fdn;
+  const double h = p->delta, h3 = pow(h, 3);
+  const double *cg = p->coeff_grad;
+  memset(floc, 0, sizeof(double) * 3 * p->n_atm);
+  memset(fcorr, 0, sizeof(double) * 3 * p->n_atm);
+  for (int r = 0; r < L->n_rep; r++) {
+    const int t = L->rep_type[r], atom = L->rep_atom[r];
+    const int *bx = L->rep_box + 6 * r;
+    const double *c = L->rep_xyz + 3 * r;
+    const int nx = bx[1] - bx[0] + 1 + 4 * fdn, ny = bx[3] - bx[2] + 1 + 4 * fdn, nz = bx[5] - bx[4] + 1 + 4 * fdn;
+    const int i0 = bx[0] - 2 * fdn, j0 = bx[2] - 2 * fdn, k0 = bx[4] - 2 * fdn;
+    const size_t nb = (size_t)nx * ny * nz;
+    double *V = malloc(sizeof(double) * nb), *Vt = malloc(sizeof(double) * nb);
+    double *bJ = calloc(nb, sizeof(double)), *bJt = calloc(nb, sizeof(double));
+    /* forces.cpp:116-143 */
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          const size_t q = ((size_t)k * ny + j) * nx + i;
+          double rad;
+          if (vloc_at(L, t, c, h, i0 + i, j0 + j, k0 + k, &V[q], &Vt[q], &rad)) {
+            free(V);
+            free(Vt);
+            free(bJ);
+            free(bJt);
+            return -1;
+          }
+        }
+    /* forces.cpp:149-173 */
+    for (int k = fdn; k < nz - fdn; k++)
+      for (int j = fdn; j < ny - fdn; j++)
+        for (int i = fdn; i < nx - fdn; i++) {
+          const size_t q = ((size_t)k * ny + j) * nx + i;
+          bJ[q] = neg_lap(p, V, nx, ny, i, j, k);
+          bJt[q] = neg_lap(p, Vt, nx, ny, i, j, k);
+        }
+    /* forces.cpp:178-277: per direction the gradients of bJ, bJ_tilda, VlocJ,
+     * VlocJ_tilda and the two force terms */
+    for (int k = 2 * fdn; k < nz - 2 * fdn; k++)
+      for (int j = 2 * fdn; j < ny - 2 * fdn; j++)
+        for (int i = 2 * fdn; i < nx - 2 * fdn; i++) {
+          const size_t q = ((size_t)k * ny + j) * nx + i;
+          const int gi = i + i0 - p->pnode_s[0], gj = j + j0 - p->pnode_s[1], gk = k + k0 - p->pnode_s[2];
+          const double ph = phi[((size_t)(gk + fdn) * PY + (gj + fdn)) * PX + (gi + fdn)];
+          const size_t g = ((size_t)gk * NY + gj) * NX + gi;
+          const size_t stride[3] = {1, (size_t)nx, (size_t)nx * ny};
+          for (int d = 0; d < 3; d++) {
+            const size_t s = stride[d];
+            double Db = 0, Dbt = 0, DV = 0, DVt = 0;
+            for (int a = 1; a <= fdn; a++) Db += (-bJ[q - a * s] + bJ[q + a * s]) * cg[a];
+            floc[3 * atom + d] += Db * (ph - V[q]) * h3;
+            for (int a = 1; a <= fdn; a++) Dbt += (-bJt[q - a * s] + bJt[q + a * s]) * cg[a];
+            for (int a = 1; a <= fdn; a++) DV += (-V[q - a * s] + V[q + a * s]) * cg[a];
+            for (int a = 1; a <= fdn; a++) DVt += (-Vt[q - a * s] + Vt[q + a * s]) * cg[a];
+            fcorr[3 * atom + d] += 0.5 *
+                                   (Dbt * (vc[g] - Vt[q]) + Db * (vc[g] + V[q]) + (DVt - DV) * (b_tilda[g] + b[g]) +
+                                    bJ[q] * DV - bJt[q] * DVt) *
+                                   h3;
+          }
+        }
+    free(V);
+    free(Vt);
+    free(bJ);
+    free(bJt);
+  }
+  return 0;
+}

@@ -82,6 +82,32 @@ int sqo_density_energy(const sqo_problem *p, const double *chi, const double *ze
 int sqo_forces_nonlocal(const sqo_problem *p, const int *nodes, int count, const double *chi, const double *zee,
                         const double *ci, double *f);
 
+/* Pseudocharge replicas of ChargeDensity and ForcesLocal: the atoms whose
+ * rb-box meets the block (Replica_atoms, initialize.cpp:21-160), in the
+ * functions' loop order (type, main atom, replica). */
+typedef struct sqo_local {
+  int n_typ;
+  const int *typ_size;            /* radial grid length per type */
+  const double *const *typ_tab;   /* per type [5][size]: grid, rVloc, DVloc, uu, Duu */
+  const double *Z;                /* valence charge per type */
+  int n_rep;
+  const int *rep_type, *rep_atom; /* replica -> type, global (type-major) atom index */
+  const double *rep_xyz;          /* [n_rep][3] */
+  const int *rep_box;             /* [n_rep][6]: xstart, xend, ystart, yend, zstart, zend (global nodes) */
+  double rc_tilda;
+} sqo_local;
+
+/* The pseudocharge part of ChargeDensity (initialize.cpp:470-784) on one
+ * block: b, b_tilda (scaled), Vc (shifted), rho_at (accumulated from zero),
+ * and scal[7] = Eself, Ncharge, Nelectron of rho_at, Ncharge_tilda,
+ * Eself_tilda, Vcon, Ecorr.  Returns 0 or -1 (spline out of range). */
+int sqo_charge_density(const sqo_problem *p, const sqo_local *L, double *b, double *b_tilda, double *vc,
+                       double *rho_at, double *scal);
+/* ForcesLocal (forces.cpp:20-315): floc and fcorr [n_atm][3] from phi (block
+ * with its FDn halo), Vc, b and b_tilda.  Returns 0 or -1. */
+int sqo_forces_local(const sqo_problem *p, const sqo_local *L, const double *phi, const double *vc, const double *b,
+                     const double *b_tilda, double *floc, double *fcorr);
+
 #ifdef __cplusplus
 }
 #endif

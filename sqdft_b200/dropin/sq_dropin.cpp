@@ -17,8 +17,9 @@
 //   SQDFT_B200_LANCZOS_TOL=T    Lanczos stop (Ha) of the two forms above
 //                               (default: the input's lanczos_tol)
 //   SQDFT_B200_DEVICE=k         CUDA device (default: MPI rank)
-//   SQDFT_B200_EXPORT=path      at the first SQ call, write the SQ inputs as a
-//                               case container (sqdft_b200/csrc/sq_case.h) and
+//   SQDFT_B200_EXPORT=path      at the first SQ call, write the SQ inputs and
+//                               the pseudocharge inputs and fields as a case
+//                               container (sqdft_b200/csrc/sq_case.h) and
 //                               exit; no GPU is touched in this mode.
 #include <cmath>
 #include <cstdio>
@@ -215,7 +216,7 @@ void ClenshawCurtisSpectralQuadrature(DS_SQ *p, int scf_iter) {
   p->mpi_time = 0.0;
   fill_veff_halo(p);
   if (export_mode()) {
-    sqb::export_case(p, std::getenv("SQDFT_B200_EXPORT"), scf_iter, false);
+    sqb::export_case(p, std::getenv("SQDFT_B200_EXPORT"), scf_iter, false, true);
     if (rank == 0) std::printf("sqdft_b200: SQ inputs written to %s\n", std::getenv("SQDFT_B200_EXPORT"));
     std::exit(0);
   }

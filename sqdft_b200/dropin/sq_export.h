@@ -10,14 +10,77 @@
 //     (Replica_atoms_Rcut, initialize.cpp:1003-1196), type-major, main atoms
 //     in input order, replicas in the reference's z-y-x image order;
 //   * per type the radial tables and spline derivatives (ds_sq.h:76-102) and
-//     the Kleinman-Bylander denominators (readfiles.cpp:1154-1216).
+//     the Kleinman-Bylander denominators (readfiles.cpp:1154-1216);
+//   * optionally (export_local) the pseudocharge inputs and fields of
+//     ChargeDensity (initialize.cpp:470-784) and ForcesLocal (forces.cpp:20-315).
 #pragma once
 #include <cmath>
+#include <string>
 #include <vector>
 
 #include "sq_case.h"
 
 namespace sqb {
+
+// Block field (np_z x np_y x np_x, with a halo of h) as a flat z-major array.
+inline std::vector<double> block_field(double ***a, int nz, int ny, int nx, int h) {
+  std::vector<double> v((size_t)(nz + 2 * h) * (ny + 2 * h) * (nx + 2 * h));
+  size_t q = 0;
+  for (int k = 0; k < nz + 2 * h; k++)
+    for (int j = 0; j < ny + 2 * h; j++)
+      for (int i = 0; i < nx + 2 * h; i++) v[q++] = a[k][j][i];
+  return v;
+}
+
+// Pseudocharge replicas (Replica_atoms, initialize.cpp:21-160: the atoms
+// whose rb-box meets the processor domain, DS_coord::ProcAtm) in the loop
+// order of ChargeDensity and ForcesLocal (type, main atom, replica): type,
+// global atom, coordinates and the intersection box; per type the radial
+// grid, rVloc, uu and their spline derivatives (getYD_gen, as both functions
+// form them) and the valence charge; rc_tilda; and the block fields as the
+// caller holds them: b, b_tilda, Vc, rho_at and phi with its FDn halo.
+inline void export_local(DS_SQ *p, CaseWriter &w) {
+  std::vector<int> rt, ra, box;
+  std::vector<double> xyz, Z;
+  int atom_count = 0;
+  for (int t = 0; t < p->n_typ; t++) {
+    Z.push_back(p->Atm[t].Z);
+    for (int a = 0; a < p->Atm[t].natm; a++, atom_count++)
+      for (int r = 0; r < p->Atm[t].Rx[a].n_replica; r++) {
+        const DS_ProcAtm &X = p->Atm[t].Rx[a].ProcAtm[r], &Y = p->Atm[t].Ry[a].ProcAtm[r],
+                         &W = p->Atm[t].Rz[a].ProcAtm[r];
+        rt.push_back(t);
+        ra.push_back(atom_count);
+        xyz.insert(xyz.end(), {X.coord, Y.coord, W.coord});
+        box.insert(box.end(), {X.start, X.end, Y.start, Y.end, W.start, W.end});
+      }
+    const int len = p->Psd[t].size;
+    std::vector<double> tab((size_t)5 * len), dv(len), du(len);
+    getYD_gen(p->Psd[t].RadialGrid, p->Psd[t].rVloc, dv.data(), len);
+    getYD_gen(p->Psd[t].RadialGrid, p->Psd[t].uu, du.data(), len);
+    for (int i = 0; i < len; i++) {
+      tab[i] = p->Psd[t].RadialGrid[i];
+      tab[(size_t)len + i] = p->Psd[t].rVloc[i];
+      tab[(size_t)2 * len + i] = dv[i];
+      tab[(size_t)3 * len + i] = p->Psd[t].uu[i];
+      tab[(size_t)4 * len + i] = du[i];
+    }
+    w.f64(("loc_tab" + std::to_string(t)).c_str(), tab.data(), {5, len});
+  }
+  const int64_t n = (int64_t)rt.size();
+  w.i32("loc_rep_type", rt.data(), {n});
+  w.i32("loc_rep_atom", ra.data(), {n});
+  w.f64("loc_rep_xyz", xyz.data(), {n, 3});
+  w.i32("loc_rep_box", box.data(), {n, 6});
+  w.f64("loc_Z", Z.data(), {p->n_typ});
+  w.f64s("loc_rc_tilda", p->rc_tilda);
+  const int nz = p->np_z, ny = p->np_y, nx = p->np_x, h = p->FDn;
+  w.f64("loc_b", block_field(p->b, nz, ny, nx, 0).data(), {nz, ny, nx});
+  w.f64("loc_b_tilda", block_field(p->b_tilda, nz, ny, nx, 0).data(), {nz, ny, nx});
+  w.f64("loc_vc", block_field(p->Vc, nz, ny, nx, 0).data(), {nz, ny, nx});
+  w.f64("loc_rho_at", block_field(p->rho_at, nz, ny, nx, 0).data(), {nz, ny, nx});
+  w.f64("loc_phi", block_field(p->phi, nz, ny, nx, h).data(), {nz + 2 * h, ny + 2 * h, nx + 2 * h});
+}
 
 inline int proj_count(const DS_SQ *p, int t) {
   int n = 0;
@@ -26,7 +89,7 @@ inline int proj_count(const DS_SQ *p, int t) {
   return n;
 }
 
-inline void export_case(DS_SQ *p, const char *path, int scf_iter, bool with_udvtm) {
+inline void export_case(DS_SQ *p, const char *path, int scf_iter, bool with_udvtm, bool with_local = false) {
   CaseWriter w(path);
   const int nl = p->nloc;
   const int ex = p->np_x + 2 * nl, ey = p->np_y + 2 * nl, ez = p->np_z + 2 * nl;
@@ -100,6 +163,7 @@ inline void export_case(DS_SQ *p, const char *path, int scf_iter, bool with_udvt
   w.f64("atoms_xyz", axyz.data(), {(int64_t)atyp.size(), 3});
   w.i32("atom_type", atyp.data(), {(int64_t)atyp.size()});
   if (with_udvtm) w.f64("udvtm", ud.data(), {(int64_t)ud.size()});
+  if (with_local) export_local(p, w);
   w.close();
 }
 
