@@ -244,6 +244,66 @@ def run_forces(args):
                       "max_abs_force": float(np.abs(f).max())}), flush=True)
 
 
+def run_local(args):
+    """Pseudocharge density and local forces of a configuration: the per-atom
+    loops of ChargeDensity (initialize.cpp:470-784) and ForcesLocal
+    (forces.cpp:20-315) through sqb_charge_density and sqb_forces_local.  W
+    untimed and S timed calls of each; device time from the library's CUDA
+    events, e2e with host buffers in and out (phi, Vc, b, b_tilda up; fields
+    and forces down).  CPU baseline: the C restatement (single thread, the
+    reference's own loops) on a sample of replicas spread over the list,
+    scaled to all of them.  Prints one JSON line."""
+    import time
+
+    from oracle.pyoracle import LocalOracle
+    from sqdft_b200 import sq
+    from sqdft_b200.case import read_container
+    from sqdft_b200.cases import make_case
+    from sqdft_b200.pseudocharge import fields_from_arrays, grid_from_arrays, local_from_arrays
+
+    a = read_container(make_case(args.config))
+    grid, loc, f = grid_from_arrays(a), local_from_arrays(a), fields_from_arrays(a)
+    cd_ms, fl_ms, wall = [], [], []
+    with sq.LocalContext(grid, loc) as ctx:
+        for _ in range(args.warmup):
+            ctx.charge_density()
+            ctx.forces_local(f["phi"], f["vc"], f["b"], f["b_tilda"])
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            cd = ctx.charge_density()
+            fl = ctx.forces_local(f["phi"], f["vc"], f["b"], f["b_tilda"])
+            wall.append((time.perf_counter() - t0) * 1e3)
+            st = ctx.stats()
+            cd_ms.append(st["ms_charge_density"])
+            fl_ms.append(st["ms_forces_local"])
+    dev_ms = float(np.mean(cd_ms) + np.mean(fl_ms))
+    n = loc.n_rep
+    line = {"mode": "local", "config": args.config, "replicas": n, "atoms": grid.n_atm,
+            "nodes": int(np.prod(grid.np_)), "charge_density_ms": float(np.mean(cd_ms)),
+            "forces_local_ms": float(np.mean(fl_ms)), "replicas_per_s": n / (dev_ms * 1e-3),
+            "e2e": {"ms": float(np.mean(wall)), "replicas_per_s": n / (float(np.mean(wall)) * 1e-3)},
+            "b_matches_export": bool(np.array_equal(cd["b"], f["b"])),
+            "max_abs_floc": float(np.abs(fl[0]).max())}
+    if not args.no_cpu:
+        # the restatement on k replicas spread over the list, per replica
+        k = min(n, args.cpu_sample or 16)
+        pick = np.unique((np.arange(k) * n) // k)
+        import dataclasses
+
+        sub = dataclasses.replace(loc, rep_type=loc.rep_type[pick], rep_atom=loc.rep_atom[pick],
+                                  rep_xyz=loc.rep_xyz[pick], rep_box=np.ascontiguousarray(loc.rep_box[pick]))
+        o = LocalOracle(grid, sub)
+        t0 = time.perf_counter()
+        o.charge_density()
+        o.forces_local(f["phi"], f["vc"], f["b"], f["b_tilda"])
+        secs = time.perf_counter() - t0
+        per = secs / len(pick)
+        line["cpu_baseline"] = {"value": 1.0 / per, "unit": "replicas/s", "cores": 1, "kind": "port",
+                                "sample": f"{len(pick)} of {n} replicas, {secs:.1f} s"}
+        line["vs_cpu"] = line["replicas_per_s"] / line["cpu_baseline"]["value"]
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args):
     if args.precision != "all" and args.sample_nodes > 0:
         return run_sample(args)
@@ -596,6 +656,8 @@ def main():
                     help="run the drop-in program's SCF loop for this many iterations on --config")
     ap.add_argument("--graph", type=int, default=2, choices=[0, 1, 2],
                     help="with --scf-steps: graph mode of the SQ step (sqb_set_graph)")
+    ap.add_argument("--local", action="store_true",
+                    help="time the pseudocharge density and local forces (sqb_charge_density, sqb_forces_local)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -603,6 +665,8 @@ def main():
         run_scf(args)
     elif args.forces_only:
         run_forces(args)
+    elif args.local:
+        run_local(args)
     else:
         run_ours(args)
 

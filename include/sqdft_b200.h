@@ -130,6 +130,8 @@ typedef struct sqb_stats {
                                    projector values a matvec reads) */
   int node_kernel;           /* kernel of the last Lanczos + moments work: SQB_KERNEL_PLANE or
                                 SQB_KERNEL_SWEEP */
+  double ms_charge_density;  /* kernels of the last sqb_charge_density */
+  double ms_forces_local;    /* kernels of the last sqb_forces_local */
 } sqb_stats;
 
 /* Create a context on CUDA device `device` (cudaSetDevice).  Mirrors the
@@ -336,6 +338,53 @@ int sqb_moments_vjp(sqb_ctx *ctx, const double *g_mu, double *g_veff, double *g_
 int sqb_density_loss(sqb_ctx *ctx, const double *w, double *loss);
 int sqb_density_loss_vjp(sqb_ctx *ctx, const double *w, int fixed_electrons, double grad_l, double *g_veff,
                          double *g_atoms);
+
+/* Pseudocharge density and local forces: the per-atom loops of
+ * ChargeDensity (initialize.cpp:470-784) and ForcesLocal (forces.cpp:20-315)
+ * on the device.  They need the block grid of the context only (delta,
+ * coeff_lap, coeff_grad, np, pnode_s; fdn 6), not Veff or the projectors. */
+
+/* One atom type of the pseudocharge: the radial tables ChargeDensity and
+ * ForcesLocal spline (DS_Psd::RadialGrid, rVloc, uu) with the derivatives
+ * getYD_gen gives them (initialize.cpp:506-510), and the valence charge. */
+typedef struct sqb_local_species {
+  int size;             /* radial grid length */
+  double Z;             /* DS_Atm::Z */
+  const double *tables; /* 5 x size rows: RadialGrid, rVloc, DVloc, uu, Duu */
+} sqb_local_species;
+
+/* The pseudocharge replicas: every atom image whose rb-box meets the block
+ * (Replica_atoms, initialize.cpp:21-160), in the reference's loop order
+ * (type, main atom, replica) as DS_Atm::R{x,y,z}[a].ProcAtm[r] lists them.
+ * rep_box[6r..6r+5] = the intersection box xstart, xend, ystart, yend, zstart,
+ * zend in global nodes (DS_ProcAtm::start/end), inside the block; rep_atom the
+ * global type-major atom index; rc_tilda the reference charge radius
+ * (DS_SQ::rc_tilda, 0.5 in ChargeDensity).  SQB_ERR_ARG for boxes outside the
+ * block, SQB_ERR_UNSUPPORTED for fdn != 6. */
+int sqb_set_local_atoms(sqb_ctx *ctx, int n_typ, const sqb_local_species *types, int n_rep, const int *rep_type,
+                        const int *rep_atom, const double *rep_xyz, const int *rep_box, double rc_tilda, int n_atm);
+
+/* ChargeDensity's pseudocharge part (initialize.cpp:470-784) on the block:
+ * b, b_tilda (scaled by |Ncharge / Ncharge_tilda|), Vc (shifted by
+ * -V000 + Vcon) and rho_at (the superposed atomic densities, from zero), each
+ * np_z x np_y x np_x z-major host arrays (any may be NULL); scal[7] =
+ * Eself, Ncharge, the integral of rho_at, Ncharge_tilda, Eself_tilda, Vcon,
+ * Ecorr.  The sums go through the allreduce hook as the reference's
+ * MPI_Allreduce (initialize.cpp:717-723, 770); V000 and Vcon come from the
+ * block that holds the main domain's first node (the reference broadcasts
+ * rank 0's).  b and rho_at equal the reference's bit for bit (each node sums
+ * its replicas in the reference's order); b_tilda and Vc to rounding (pow).
+ * The initial-guess handling of rho (MD step, restart, charge extrapolation)
+ * stays with the caller. */
+int sqb_charge_density(sqb_ctx *ctx, double *b, double *b_tilda, double *vc, double *rho_at, double *scal);
+
+/* ForcesLocal (forces.cpp:20-315): the block's local forces floc and the
+ * overlap-correction forces fcorr, [n_atm][3] host arrays, from phi (the
+ * block with its fdn halo, (np_z+2fdn) x (np_y+2fdn) x (np_x+2fdn)), Vc, b and
+ * b_tilda (block arrays).  Like the reference the result is this block's
+ * part (no reduction across ranks). */
+int sqb_forces_local(sqb_ctx *ctx, const double *phi, const double *vc, const double *b, const double *b_tilda,
+                     double *floc, double *fcorr);
 
 /* Size of the fixed device scratch array used by sqb_lanczos_moments_noalloc
  * (held on every GPU that loads the library, until the process exits). */

@@ -22,10 +22,11 @@ LIB = BUILD / "libsqdft_b200.so"
 INCLUDE = HERE.parent / "include"
 
 SOURCES = ["sqb_api.cu", "sqb_node.cu", "sqb_node_forces.cu", "sqb_node_vjp.cu", "sqb_node_mixed.cu", "sqb_node_lq.cu",
-           "sqb_fermi.cu", "sqb_sweep.cu", "sqb_sweep_forces.cu", "sqb_fermi_dev.cu"]
+           "sqb_fermi.cu", "sqb_sweep.cu", "sqb_sweep_forces.cu", "sqb_fermi_dev.cu", "sqb_local.cu"]
 # Sources that need flags of their own: the device-side Fermi solver rounds
-# every operation as the host solver does (no multiply-add contraction).
-EXTRA = {"sqb_fermi_dev.cu": ["-fmad=false"]}
+# every operation as the host solver does, and the pseudocharge kernels as
+# the reference's x86 build does (no multiply-add contraction).
+EXTRA = {"sqb_fermi_dev.cu": ["-fmad=false"], "sqb_local.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -104,6 +104,20 @@ struct sqb_ctx {
   std::string metrics_path;  // SQDFT_B200_METRICS at creation: one JSON line per SQ step / force pass
   unsigned test_extra_tx = 0;           // sqb_test_stage_wait
   unsigned long long test_wait_ns = 0;
+
+  // pseudocharge replicas (sqb_set_local_atoms) and the block fields of
+  // sqb_charge_density / sqb_forces_local
+  int loc_nrep = 0, loc_natm = 0;
+  double loc_rc_tilda = 0.0;
+  bool have_local = false;
+  std::vector<int> h_loc_atom, h_loc_box;
+  int *d_loc_type = nullptr, *d_loc_atom = nullptr, *d_loc_box = nullptr, *d_loc_size = nullptr;
+  long long *d_loc_off = nullptr, *d_loc_scr_off = nullptr;
+  double *d_loc_xyz = nullptr, *d_loc_tab = nullptr, *d_loc_Z = nullptr;
+  double *d_loc_fields = nullptr;  // b, b_tilda, Vc, rho_at, phi (+halo), partial sums
+  size_t loc_fields_bytes = 0;
+  double *d_loc_scr = nullptr;     // ForcesLocal scratch boxes and per-CTA force sums
+  size_t loc_scr_bytes = 0;
 };
 
 namespace {
@@ -779,7 +793,9 @@ int sqb_destroy(sqb_ctx *c) {
                   c->d_tables, c->d_rep_xyz, c->d_rep_off_ref, c->d_vjp, c->d_vjp_at, c->d_dtab, c->d_tab64, c->d_scratch, c->d_counter, c->d_nodes,
                   c->d_status, c->d_iters, c->d_proj_points, c->d_chi, c->d_zee, c->d_rho_pj, c->d_lmin,
                   c->d_lmax, c->d_xk, c->d_ctab, c->d_partial, c->d_result, c->d_rho, c->d_ci, c->d_fslots,
-                  c->d_f, c->d_tmp, c->d_sens, c->d_loss, c->d_fermi};
+                  c->d_f, c->d_tmp, c->d_sens, c->d_loss, c->d_fermi, c->d_loc_type, c->d_loc_atom,
+                  c->d_loc_box, c->d_loc_size, c->d_loc_off, c->d_loc_scr_off, c->d_loc_xyz, c->d_loc_tab,
+                  c->d_loc_Z, c->d_loc_fields, c->d_loc_scr};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   drop_graph(c);
@@ -2056,6 +2072,278 @@ int sqb_lanczos_moments_noalloc(sqb_ctx *c, int count, const int *nodes, double 
 int sqb_get_stats(const sqb_ctx *c, sqb_stats *out, size_t out_size) {
   if (!c || !out || out_size == 0) return SQB_ERR_ARG;
   std::memcpy(out, &c->stats, out_size < sizeof(sqb_stats) ? out_size : sizeof(sqb_stats));
+  return SQB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Pseudocharge density and local forces (sqb_local.cu)
+
+namespace {
+
+LocalArgs local_args(const sqb_ctx *c) {
+  LocalArgs a{};
+  for (int d = 0; d < 3; d++) {
+    a.np[d] = c->g.np[d];
+    a.pnode_s[d] = c->g.pnode_s[d];
+  }
+  a.delta = c->g.delta;
+  a.h3 = c->h3;  // pow(delta, 3), as the reference forms it
+  for (int k = 0; k <= FDN; k++) {
+    a.coeff_lap[k] = c->g.coeff_lap[k];
+    a.coeff_grad[k] = c->g.coeff_grad[k];
+  }
+  a.n_rep = c->loc_nrep;
+  a.rep_type = c->d_loc_type;
+  a.rep_atom = c->d_loc_atom;
+  a.rep_xyz = c->d_loc_xyz;
+  a.rep_box = c->d_loc_box;
+  a.tab = c->d_loc_tab;
+  a.typ_off = c->d_loc_off;
+  a.typ_size = c->d_loc_size;
+  a.Z = c->d_loc_Z;
+  a.rc_tilda = c->loc_rc_tilda;
+  a.status = c->d_status;
+  return a;
+}
+
+// Block fields of the pseudocharge calls: b, b_tilda, Vc, rho_at (N each),
+// phi with its FDN halo, and the per-CTA sums.
+int ensure_local_fields(sqb_ctx *c, double **f, double **phi, double **partial) {
+  const size_t N = (size_t)c->nnode;
+  const size_t P = (size_t)(c->g.np[0] + 2 * FDN) * (c->g.np[1] + 2 * FDN) * (c->g.np[2] + 2 * FDN);
+  const size_t parts = (size_t)5 * charge_density_ctas(c->g.np);
+  const size_t need = (4 * N + P + parts) * sizeof(double);
+  if (c->loc_fields_bytes < need) {
+    if (c->d_loc_fields) cudaFree(c->d_loc_fields);
+    c->d_loc_fields = nullptr;
+    CK(cudaMalloc((void **)&c->d_loc_fields, need));
+    c->loc_fields_bytes = need;
+  }
+  *f = c->d_loc_fields;
+  *phi = c->d_loc_fields + 4 * N;
+  *partial = *phi + P;
+  return SQB_OK;
+}
+
+// Sum of a device array of n doubles in index order, on the host.
+int host_sum(sqb_ctx *c, const double *d, size_t n, int stride_count, double *out) {
+  std::vector<double> h(n * (size_t)stride_count);
+  CK(cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < stride_count; k++) {
+    double s = 0.0;
+    for (size_t i = 0; i < n; i++) s += h[(size_t)k * n + i];
+    out[k] = s;
+  }
+  return SQB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sqb_set_local_atoms(sqb_ctx *c, int n_typ, const sqb_local_species *types, int n_rep, const int *rep_type,
+                        const int *rep_atom, const double *rep_xyz, const int *rep_box, double rc_tilda, int n_atm) {
+  if (!c || n_typ <= 0 || !types || n_rep < 0 || n_atm <= 0 || !(rc_tilda > 0)) return SQB_ERR_ARG;
+  if (n_rep > 0 && (!rep_type || !rep_atom || !rep_xyz || !rep_box)) return SQB_ERR_ARG;
+  if (c->g.fdn != FDN) return SQB_ERR_UNSUPPORTED;
+  cudaSetDevice(c->device);
+  std::vector<long long> off(n_typ);
+  std::vector<int> size(n_typ);
+  std::vector<double> Z(n_typ);
+  long long total = 0;
+  for (int t = 0; t < n_typ; t++) {
+    if (types[t].size < 2 || !types[t].tables) return SQB_ERR_ARG;
+    off[t] = total;
+    size[t] = types[t].size;
+    Z[t] = types[t].Z;
+    total += 5LL * types[t].size;
+  }
+  for (int r = 0; r < n_rep; r++) {
+    if (rep_type[r] < 0 || rep_type[r] >= n_typ || rep_atom[r] < 0 || rep_atom[r] >= n_atm) return SQB_ERR_ARG;
+    for (int d = 0; d < 3; d++) {
+      const int lo = rep_box[6 * r + 2 * d], hi = rep_box[6 * r + 2 * d + 1];
+      if (lo > hi || lo < c->g.pnode_s[d] || hi >= c->g.pnode_s[d] + c->g.np[d]) return SQB_ERR_ARG;
+    }
+  }
+  std::vector<double> tab((size_t)std::max<long long>(total, 1));
+  for (int t = 0; t < n_typ; t++)
+    std::memcpy(&tab[(size_t)off[t]], types[t].tables, sizeof(double) * 5 * (size_t)types[t].size);
+  const size_t nr = (size_t)std::max(n_rep, 1);
+  CK(dalloc(&c->d_loc_tab, tab.size()));
+  CK(dalloc(&c->d_loc_off, (size_t)n_typ));
+  CK(dalloc(&c->d_loc_size, (size_t)n_typ));
+  CK(dalloc(&c->d_loc_Z, (size_t)n_typ));
+  CK(dalloc(&c->d_loc_type, nr));
+  CK(dalloc(&c->d_loc_atom, nr));
+  CK(dalloc(&c->d_loc_xyz, 3 * nr));
+  CK(dalloc(&c->d_loc_box, 6 * nr));
+  CK(cudaMemcpy(c->d_loc_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_loc_off, off.data(), n_typ * sizeof(long long), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_loc_size, size.data(), n_typ * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_loc_Z, Z.data(), n_typ * sizeof(double), cudaMemcpyHostToDevice));
+  if (n_rep > 0) {
+    CK(cudaMemcpy(c->d_loc_type, rep_type, n_rep * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_loc_atom, rep_atom, n_rep * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_loc_xyz, rep_xyz, 3 * (size_t)n_rep * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_loc_box, rep_box, 6 * (size_t)n_rep * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  c->h_loc_atom.assign(rep_atom, rep_atom + n_rep);
+  c->h_loc_box.assign(rep_box, rep_box + 6 * (size_t)n_rep);
+  c->loc_nrep = n_rep;
+  c->loc_natm = n_atm;
+  c->loc_rc_tilda = rc_tilda;
+  c->have_local = true;
+  return SQB_OK;
+}
+
+int sqb_charge_density(sqb_ctx *c, double *b, double *b_tilda, double *vc, double *rho_at, double *scal) {
+  if (!c || !scal) return SQB_ERR_ARG;
+  if (!c->have_local) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  NvtxRange nr("sqb_charge_density");
+  const size_t N = (size_t)c->nnode;
+  double *f = nullptr, *phi = nullptr, *partial = nullptr;
+  int rc = ensure_local_fields(c, &f, &phi, &partial);
+  if (rc) return rc;
+  LocalArgs a = local_args(c);
+  a.b = f;
+  a.b_tilda = f + N;
+  a.vc = f + 2 * N;
+  a.rho_at = f + 3 * N;
+  a.partial = partial;
+  const int ncta = charge_density_ctas(c->g.np);
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  CK(cudaEventRecord(c->ev0, c->stream));
+  CK(launch_charge_density(a, c->stream));
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  // sums in CTA order: Eself, Ncharge, integral of rho_at, Ncharge_tilda, Eself_tilda
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};
+  rc = host_sum(c, partial, (size_t)ncta, 5, v);
+  if (rc) return rc;
+  rc = status_to_err(st);
+  if (rc) return rc;
+  // V000 (rank 0's Vc[0][0][0]) and Vcon (Vt - V summed at the main
+  // domain's first node over the replicas that hold it, initialize.cpp:631-635)
+  // both come from the block that starts at the main domain's first node: the
+  // unshifted Vc there is the same sum in the same order.  Other blocks add 0.
+  const int *ps = c->g.pnode_s;
+  if (ps[0] == 0 && ps[1] == 0 && ps[2] == 0) {
+    double v0 = 0.0;
+    CK(cudaMemcpyAsync(&v0, a.vc, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    v[5] = v0;
+    v[6] = v0;
+  }
+  rc = reduce(c, v, 7, SQB_SUM);  // initialize.cpp:717-723 and the broadcasts of :741-742
+  if (rc) return rc;
+  const double scale = fabs(v[1] / v[3]), shift = -v[5] + v[6];
+  CK(launch_charge_finish(a, scale, shift, c->stream));
+  CK(cudaEventRecord(c->ev1, c->stream));
+  double ecorr = 0.0;
+  rc = host_sum(c, partial, (size_t)ncta, 1, &ecorr);
+  if (rc) return rc;
+  rc = reduce(c, &ecorr, 1, SQB_SUM);  // initialize.cpp:770
+  if (rc) return rc;
+  c->stats.ms_charge_density = elapsed(c);
+  double *outs[4] = {b, b_tilda, vc, rho_at};
+  for (int k = 0; k < 4; k++)
+    if (outs[k]) CK(cudaMemcpyAsync(outs[k], f + k * N, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  scal[0] = v[0];
+  scal[1] = v[1];
+  scal[2] = v[2];
+  scal[3] = v[3];
+  scal[4] = v[4];
+  scal[5] = v[6];
+  scal[6] = ecorr + v[0] - v[4];  // Ecorr_global + Eself - Eself_tilda (initialize.cpp:775)
+  return SQB_OK;
+}
+
+int sqb_forces_local(sqb_ctx *c, const double *phi, const double *vc, const double *b, const double *b_tilda,
+                     double *floc, double *fcorr) {
+  if (!c || !phi || !vc || !b || !b_tilda || !floc || !fcorr) return SQB_ERR_ARG;
+  if (!c->have_local) return SQB_ERR_STATE;
+  cudaSetDevice(c->device);
+  NvtxRange nr("sqb_forces_local");
+  const size_t N = (size_t)c->nnode;
+  const size_t P = (size_t)(c->g.np[0] + 2 * FDN) * (c->g.np[1] + 2 * FDN) * (c->g.np[2] + 2 * FDN);
+  double *f = nullptr, *d_phi = nullptr, *partial = nullptr;
+  int rc = ensure_local_fields(c, &f, &d_phi, &partial);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(d_phi, phi, P * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(f, b, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(f + N, b_tilda, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(f + 2 * N, vc, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  LocalArgs a = local_args(c);
+  a.phi = d_phi;
+  a.bf = f;
+  a.btf = f + N;
+  a.vcf = f + 2 * N;
+  // replicas in batches whose scratch boxes (4 fields each, box + 2 fdn
+  // per side) fit 1 GiB
+  const int n = c->loc_nrep;
+  std::vector<long long> vol(n);
+  for (int r = 0; r < n; r++) {
+    const int *bx = &c->h_loc_box[6 * (size_t)r];
+    vol[r] = (long long)(bx[1] - bx[0] + 1 + 4 * FDN) * (bx[3] - bx[2] + 1 + 4 * FDN) * (bx[5] - bx[4] + 1 + 4 * FDN);
+  }
+  const long long budget = (1LL << 30) / (long long)sizeof(double);
+  std::vector<double> fsum((size_t)6 * c->loc_natm, 0.0);
+  CK(dalloc(&c->d_loc_scr_off, (size_t)std::max(n, 1)));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+  CK(cudaEventRecord(c->ev0, c->stream));
+  for (int r0 = 0; r0 < n;) {
+    int r1 = r0;
+    long long used = 0;
+    std::vector<long long> offs;
+    while (r1 < n && (r1 == r0 || used + 4 * vol[r1] <= budget)) {
+      offs.push_back(used);
+      used += 4 * vol[r1];
+      r1++;
+    }
+    const size_t nb = (size_t)(r1 - r0);
+    const size_t need = (size_t)used * sizeof(double) + nb * LOC_FORCE_CTAS * 6 * sizeof(double);
+    if (c->loc_scr_bytes < need) {
+      if (c->d_loc_scr) cudaFree(c->d_loc_scr);
+      c->d_loc_scr = nullptr;
+      CK(cudaMalloc((void **)&c->d_loc_scr, need));
+      c->loc_scr_bytes = need;
+    }
+    // the kernels index the scratch by replica: offsets of [r0, r1) at slots r0..
+    CK(cudaMemcpyAsync(c->d_loc_scr_off + r0, offs.data(), nb * sizeof(long long), cudaMemcpyHostToDevice,
+                       c->stream));
+    a.scr = c->d_loc_scr;
+    a.scr_off = c->d_loc_scr_off;
+    a.fpart = c->d_loc_scr + used;
+    CK(launch_forces_local(a, r0, r1, c->stream));
+    std::vector<double> part(nb * LOC_FORCE_CTAS * 6);
+    CK(cudaMemcpyAsync(part.data(), a.fpart, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < nb; i++) {
+      double rs[6] = {0, 0, 0, 0, 0, 0};
+      for (int k = 0; k < LOC_FORCE_CTAS; k++)
+        for (int q = 0; q < 6; q++) rs[q] += part[(i * LOC_FORCE_CTAS + k) * 6 + q];
+      const int atom = c->h_loc_atom[r0 + i];
+      for (int q = 0; q < 6; q++) fsum[(size_t)6 * atom + q] += rs[q];
+    }
+    r0 = r1;
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->stats.ms_forces_local = elapsed(c);
+  rc = status_to_err(st);
+  if (rc) return rc;
+  for (int at = 0; at < c->loc_natm; at++)
+    for (int d = 0; d < 3; d++) {
+      floc[3 * at + d] = fsum[(size_t)6 * at + d];
+      fcorr[3 * at + d] = fsum[(size_t)6 * at + 3 + d];
+    }
   return SQB_OK;
 }
 

@@ -283,4 +283,44 @@ cudaError_t launch_repack(int n_rep, const int *rep_nn, const int *typ_nlocc, co
                           int to_pad, cudaStream_t s);
 cudaError_t launch_minmax(const double *lmin, const double *lmax, int n, double *out, cudaStream_t s);
 
+// Pseudocharge density and local forces (sqb_local.cu): ChargeDensity
+// (initialize.cpp:470-784) and ForcesLocal (forces.cpp:20-315) on the block.
+struct LocalArgs {
+  int np[3], pnode_s[3];
+  double delta, h3;  // h3 = pow(delta, 3) formed on the host
+  double coeff_lap[FDN + 1], coeff_grad[FDN + 1];
+  int n_rep;
+  const int *rep_type, *rep_atom;
+  const double *rep_xyz;  // [n_rep][3]
+  const int *rep_box;     // [n_rep][6]: xstart, xend, ystart, yend, zstart, zend (global nodes)
+  const double *tab;      // per type [5][size]: grid, rVloc, DVloc, uu, Duu
+  const long long *typ_off;
+  const int *typ_size;
+  const double *Z;
+  double rc_tilda;
+  int *status;
+  // ChargeDensity: block fields (raw: b_tilda unscaled, Vc unshifted) and
+  // per-CTA sums [5][n_cta] of Eself, Ncharge, the rho_at integral,
+  // Ncharge_tilda, Eself_tilda
+  double *b, *b_tilda, *vc, *rho_at, *partial;
+  // ForcesLocal: the fields it reads (phi with its FDN halo), the per-replica
+  // scratch boxes (VlocJ, VlocJ_tilda, bJ, bJ_tilda, each box + 2 FDN wide)
+  // at scr + scr_off[r], and per-(replica, CTA) force sums [6]
+  const double *phi, *vcf, *bf, *btf;
+  double *scr;
+  const long long *scr_off;
+  double *fpart;
+};
+// Tile edge of the charge-density kernel and its CTA count for the block.
+constexpr int LOC_TILE = 8;
+int charge_density_ctas(const int np[3]);
+cudaError_t launch_charge_density(const LocalArgs &a, cudaStream_t s);
+// b_tilda *= scale, Vc += shift, and per-CTA sums of 0.5 (b_tilda + b) Vc h^3
+// into partial[0..n_cta) (the Ecorr loop of initialize.cpp:759-768).
+cudaError_t launch_charge_finish(const LocalArgs &a, double scale, double shift, cudaStream_t s);
+constexpr int LOC_FORCE_CTAS = 64;  // CTAs per replica of the force contraction
+// ForcesLocal for replicas [r0, r1): scratch boxes, then per-(replica, CTA)
+// force sums into fpart[((r - r0) * LOC_FORCE_CTAS + cta) * 6].
+cudaError_t launch_forces_local(const LocalArgs &a, int r0, int r1, cudaStream_t s);
+
 }  // namespace sqb

@@ -40,8 +40,13 @@ EXPORTS = [
     "sqb_lanczos_moments_noalloc", "sqb_moments_at", "sqb_moments_vjp", "sqb_autotune",
     "sqb_set_graph", "sqb_set_mixed_lanczos", "sqb_set_defect_check", "sqb_lanczos_moments_nodes",
     "sqb_set_node_kernel", "sqb_set_veff_device", "sqb_test_stage_wait", "sqb_density_loss",
-    "sqb_density_loss_vjp", "sqb_set_sweep_rows", "sqb_autotune_sweep",
+    "sqb_density_loss_vjp", "sqb_set_sweep_rows", "sqb_autotune_sweep", "sqb_set_local_atoms",
+    "sqb_charge_density", "sqb_forces_local",
 ]
+
+
+class SqbLocalSpecies(C.Structure):
+    _fields_ = [("size", C.c_int), ("Z", C.c_double), ("tables", _dp)]
 
 
 class SqbGrid(C.Structure):
@@ -64,7 +69,7 @@ class SqbStats(C.Structure):
                 ("fermi_iters", C.c_int), ("max_lanczos_iters", C.c_int), ("kernel_launches", C.c_int),
                 ("ms_vjp", C.c_double), ("ms_defect", C.c_double), ("defect_nodes", C.c_longlong),
                 ("lanczos_maxiter_nodes", C.c_longlong), ("proj_points_window", C.c_longlong),
-                ("node_kernel", C.c_int)]
+                ("node_kernel", C.c_int), ("ms_charge_density", C.c_double), ("ms_forces_local", C.c_double)]
 
 
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, _dp, C.c_int, C.c_int, C.c_void_p)
@@ -119,6 +124,10 @@ def library() -> C.CDLL:
         lib.sqb_autotune_sweep.argtypes = [P, C.c_int, _ip, _dp]
         lib.sqb_density_loss_vjp.argtypes = [P, _dp, C.c_int, C.c_double, _dp, _dp]
         lib.sqb_moments_vjp.argtypes = [P, _dp, _dp, _dp]
+        lib.sqb_set_local_atoms.argtypes = [P, C.c_int, C.POINTER(SqbLocalSpecies), C.c_int, _ip, _ip, _dp, _ip,
+                                            C.c_double, C.c_int]
+        lib.sqb_charge_density.argtypes = [P, _dp, _dp, _dp, _dp, _dp]
+        lib.sqb_forces_local.argtypes = [P, _dp, _dp, _dp, _dp, _dp, _dp]
         lib.sqb_status_string.argtypes = [C.c_int]
         lib.sqb_status_string.restype = C.c_char_p
         lib.sqb_version.restype = C.c_char_p
@@ -166,6 +175,7 @@ class Context:
             self.set_allreduce(allreduce)
         self.set_precision(precision)
         self._keep = []
+        self.local_shape = tuple(case.np_[::-1])
         self.set_veff(case.veff)
         self.set_atoms(case)
 
@@ -407,6 +417,95 @@ class Context:
         _check(self.lib.sqb_forces_nonlocal(self.ptr, _d(args[0]), _d(args[1]), _d(args[2]), _d(f)),
                "sqb_forces_nonlocal")
         return f
+
+    def stats(self) -> dict:
+        s = SqbStats()
+        _check(self.lib.sqb_get_stats(self.ptr, C.byref(s), C.sizeof(s)), "sqb_get_stats")
+        return {k: getattr(s, k) for k, _ in SqbStats._fields_}
+
+    # -- pseudocharge density and local forces ---------------------------------
+    def set_local_atoms(self, loc, n_atm: int | None = None):
+        """sqb_set_local_atoms with a :class:`sqdft_b200.pseudocharge.LocalAtoms`."""
+        _set_local_atoms(self, loc, self.case.n_atm if n_atm is None else n_atm)
+
+    def charge_density(self) -> dict:
+        """sqb_charge_density: ChargeDensity's pseudocharge part (initialize.cpp:470-784)."""
+        return _charge_density(self)
+
+    def forces_local(self, phi, vc, b, b_tilda):
+        """sqb_forces_local (forces.cpp:20-315): (floc, fcorr), [n_atm, 3] each."""
+        return _forces_local(self, phi, vc, b, b_tilda)
+
+
+def _set_local_atoms(ctx, loc, n_atm: int) -> None:
+    tabs = [np.ascontiguousarray(t, np.float64) for t in loc.tables]
+    sp = (SqbLocalSpecies * len(tabs))()
+    for t, tab in enumerate(tabs):
+        sp[t].size, sp[t].Z, sp[t].tables = tab.shape[1], float(loc.Z[t]), _d(tab)
+    arrs = (np.ascontiguousarray(loc.rep_type, np.int32), np.ascontiguousarray(loc.rep_atom, np.int32),
+            np.ascontiguousarray(loc.rep_xyz, np.float64), np.ascontiguousarray(loc.rep_box, np.int32))
+    _check(ctx.lib.sqb_set_local_atoms(ctx.ptr, len(tabs), sp, len(arrs[0]), _i(arrs[0]), _i(arrs[1]), _d(arrs[2]),
+                                       _i(arrs[3]), float(loc.rc_tilda), int(n_atm)), "sqb_set_local_atoms")
+    ctx._local_natm = int(n_atm)
+
+
+def _charge_density(ctx) -> dict:
+    sh = tuple(ctx.local_shape)
+    b, bt, vc, ra = (np.zeros(sh) for _ in range(4))
+    scal = np.zeros(7)
+    _check(ctx.lib.sqb_charge_density(ctx.ptr, _d(b), _d(bt), _d(vc), _d(ra), _d(scal)), "sqb_charge_density")
+    return dict(b=b, b_tilda=bt, vc=vc, rho_at=ra, Eself=scal[0], Ncharge=scal[1], Nelectron_at=scal[2],
+                Ncharge_tilda=scal[3], Eself_tilda=scal[4], Vcon=scal[5], Ecorr=scal[6])
+
+
+def _forces_local(ctx, phi, vc, b, b_tilda):
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (phi, vc, b, b_tilda)]
+    n = ctx._local_natm
+    floc, fcorr = np.zeros((n, 3)), np.zeros((n, 3))
+    _check(ctx.lib.sqb_forces_local(ctx.ptr, *[_d(a) for a in arrs], _d(floc), _d(fcorr)), "sqb_forces_local")
+    return floc, fcorr
+
+
+class LocalContext:
+    """An sqb_ctx used for the pseudocharge calls only: the block grid of a
+    :class:`sqdft_b200.pseudocharge.LocalGrid` and the replicas of a
+    :class:`~sqdft_b200.pseudocharge.LocalAtoms` (no Veff or projectors)."""
+
+    def __init__(self, grid, loc, device: int = 0, allreduce=None):
+        self.lib = library()
+        g = SqbGrid()
+        g.np[:] = list(grid.np_)
+        g.pnode_s[:] = list(grid.pnode_s)
+        g.n_int[:] = list(grid.np_)
+        g.nloc, g.fdn, g.npl, g.fermi_alg = 1, grid.fdn, 4, 1
+        g.delta, g.bet, g.lanczos_tol, g.fermi_tol, g.ncharge = grid.delta, 1.0, 1e-6, 1e-6, 0.0
+        for k in range(grid.fdn + 1):
+            g.coeff_lap[k] = float(grid.coeff_lap[k])
+            g.coeff_grad[k] = float(grid.coeff_grad[k])
+        self.ptr = C.c_void_p()
+        _check(self.lib.sqb_create(C.byref(g), device, C.byref(self.ptr)), "sqb_create")
+        self.local_shape = tuple(grid.np_[::-1])
+        self._cb = None
+        if allreduce is not None:
+            Context.set_allreduce(self, allreduce)
+        _set_local_atoms(self, loc, grid.n_atm)
+
+    def close(self):
+        if self.ptr:
+            self.lib.sqb_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def charge_density(self) -> dict:
+        return _charge_density(self)
+
+    def forces_local(self, phi, vc, b, b_tilda):
+        return _forces_local(self, phi, vc, b, b_tilda)
 
     def stats(self) -> dict:
         s = SqbStats()
