@@ -7,7 +7,11 @@
 //   ClenshawCurtisSpectralQuadrature(DS_SQ*, int)  func_sq.h:515, sq.cpp:377
 //   NonlocalProjectors(DS_SQ*)                     func_sq.h:368, nonlocal.cpp:317
 //   ForcesNonLocal(DS_SQ*)                         func_sq.h:540, forces.cpp:318
-// (the reference definitions are weakened in their objects, see Makefile).
+// (the reference definitions are weakened in their objects, see Makefile),
+// and, with SQDFT_B200_LOCAL=1, the per-atom loops of
+//   ChargeDensity(DS_SQ*)                          func_sq.h:133, initialize.cpp:470
+//   ForcesLocal(DS_SQ*)                            func_sq.h:534, forces.cpp:20
+// (otherwise the reference's own, kept as ref_ChargeDensity / ref_ForcesLocal).
 // It reads and writes the same DS_SQ fields as the functions it replaces.
 // Failures print the reference's message and exit(1), as the reference does.
 //
@@ -17,6 +21,7 @@
 //   SQDFT_B200_LANCZOS_TOL=T    Lanczos stop (Ha) of the two forms above
 //                               (default: the input's lanczos_tol)
 //   SQDFT_B200_DEVICE=k         CUDA device (default: MPI rank)
+//   SQDFT_B200_LOCAL=1          pseudocharge density and local forces on the GPU
 //   SQDFT_B200_EXPORT=path      at the first SQ call, write the SQ inputs and
 //                               the pseudocharge inputs and fields as a case
 //                               container (sqdft_b200/csrc/sq_case.h) and
@@ -267,5 +272,132 @@ void ForcesNonLocal(DS_SQ *p) {
     p->fnlocx[a] = f[3 * a];
     p->fnlocy[a] = f[3 * a + 1];
     p->fnlocz[a] = f[3 * a + 2];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ChargeDensity and ForcesLocal.  By default the reference's own functions
+// run (kept in the program under the names ref_ChargeDensity and
+// ref_ForcesLocal, see Makefile); with SQDFT_B200_LOCAL=1 their per-atom
+// loops run on the GPU (sqb_charge_density, sqb_forces_local) and the rest
+// of ChargeDensity -- the initial density guess, its scaling to the nuclear
+// charge, the Poisson right-hand side -- follows here on the host as
+// initialize.cpp:637-784 does.  Export mode always runs the reference path.
+
+void ref_ChargeDensity(DS_SQ *p);  // initialize.cpp:470 (renamed)
+void ref_ForcesLocal(DS_SQ *p);    // forces.cpp:20 (renamed)
+
+namespace {
+
+bool local_on_device() {
+  const char *v = std::getenv("SQDFT_B200_LOCAL");
+  return v && !std::strcmp(v, "1") && !export_mode();
+}
+
+void upload_local_atoms(DS_SQ *p) {
+  const sqb::LocalInputs L = sqb::gather_local(p);
+  std::vector<sqb_local_species> sp(p->n_typ);
+  for (int t = 0; t < p->n_typ; t++) {
+    sp[t].size = (int)(L.tables[t].size() / 5);
+    sp[t].Z = L.Z[t];
+    sp[t].tables = L.tables[t].data();
+  }
+  const int rc = sqb_set_local_atoms(g_ctx, p->n_typ, sp.data(), (int)L.rep_type.size(), L.rep_type.data(),
+                                     L.rep_atom.data(), L.rep_xyz.data(), L.rep_box.data(), p->rc_tilda, p->n_atm);
+  if (rc) fail(rc, "local atoms");
+}
+
+void put_block(double ***a, const std::vector<double> &v, int nz, int ny, int nx) {
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++) std::memcpy(a[k][j], &v[((size_t)k * ny + j) * nx], sizeof(double) * nx);
+}
+
+}  // namespace
+
+void ChargeDensity(DS_SQ *p) {
+  if (!local_on_device()) {
+    ref_ChargeDensity(p);
+    return;
+  }
+  int rank = 0;
+  MPI_Comm_rank(MPI_COMM_WORLD, &rank);
+  ensure_ctx(p);
+  p->rc_tilda = 0.5;  // initialize.cpp:483
+  upload_local_atoms(p);
+  const int nz = p->np_z, ny = p->np_y, nx = p->np_x;
+  const size_t N = (size_t)nz * ny * nx;
+  std::vector<double> b(N), bt(N), vc(N), ra(N);
+  double scal[7];
+  int rc = sqb_charge_density(g_ctx, b.data(), bt.data(), vc.data(), ra.data(), scal);
+  if (rc) fail(rc, "ChargeDensity");
+  // b, the scaled b_tilda and the shifted Vc replace the block's; rho_at
+  // accumulates as the reference's loop adds into it (initialize.cpp:585)
+  put_block(p->b, b, nz, ny, nx);
+  put_block(p->b_tilda, bt, nz, ny, nx);
+  put_block(p->Vc, vc, nz, ny, nx);
+  size_t q = 0;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) p->rho_at[k][j][i] += ra[q++];
+  p->Eself = scal[0];
+  p->Ncharge = scal[1];
+  // the density guess: rho_at on the first MD step, a restart file, or the
+  // extrapolated density from the fourth MD step on (initialize.cpp:637-694)
+  if (p->MDstepCount == 1)
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++) std::memcpy(p->rho[k][j], p->rho_at[k][j], sizeof(double) * nx);
+  if (p->restart_scf == 1) RestartSCF(p);
+  if (p->MDstepCount > 3 && p->ChgExtrap == 1) {
+    if (rank == 0) std::printf("Using Charge extrapolation for rho_guess! \n");
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          p->rho[k][j][i] = p->rho_at[k][j][i] + p->drho_new[k][j][i];
+          if (p->rho[k][j][i] < 0.0) p->rho[k][j][i] = pow(10.0, -6.0);
+        }
+  }
+  double nel = 0.0;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) nel += p->rho[k][j][i] * p->delta * p->delta * p->delta;
+  MPI_Allreduce(MPI_IN_PLACE, &nel, 1, MPI_DOUBLE, MPI_SUM, MPI_COMM_WORLD);
+  // scale rho to the nuclear charge (initialize.cpp:728-739)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) p->rho[k][j][i] = fabs(p->Ncharge / nel) * p->rho[k][j][i];
+  p->Nelectron = -p->Ncharge;
+  // Poisson right-hand side and the first MD step's phi guess
+  // (initialize.cpp:755-767; the whole block)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        if (p->MDstepCount == 1) p->phi_guess[k + p->FDn][j + p->FDn][i + p->FDn] = 1;
+        p->rhs[k][j][i] = p->b[k][j][i] + p->rho[k][j][i];
+      }
+  p->Ecorr = scal[6];
+  if (p->Correction == 1 && rank == 0) std::printf("Energy Correction (Ha/atom) : %.14f \n", p->Ecorr / p->n_atm);
+}
+
+void ForcesLocal(DS_SQ *p) {
+  if (!local_on_device()) {
+    ref_ForcesLocal(p);
+    return;
+  }
+  ensure_ctx(p);
+  upload_local_atoms(p);
+  const int nz = p->np_z, ny = p->np_y, nx = p->np_x;
+  const std::vector<double> phi = sqb::block_field(p->phi, nz, ny, nx, p->FDn);
+  const std::vector<double> vc = sqb::block_field(p->Vc, nz, ny, nx, 0), b = sqb::block_field(p->b, nz, ny, nx, 0),
+                            bt = sqb::block_field(p->b_tilda, nz, ny, nx, 0);
+  std::vector<double> fl((size_t)3 * p->n_atm), fc((size_t)3 * p->n_atm);
+  const int rc = sqb_forces_local(g_ctx, phi.data(), vc.data(), b.data(), bt.data(), fl.data(), fc.data());
+  if (rc) fail(rc, "ForcesLocal");
+  for (int a = 0; a < p->n_atm; a++) {
+    p->flocx[a] = fl[3 * a];
+    p->flocy[a] = fl[3 * a + 1];
+    p->flocz[a] = fl[3 * a + 2];
+    p->fcorrx[a] = fc[3 * a];
+    p->fcorry[a] = fc[3 * a + 1];
+    p->fcorrz[a] = fc[3 * a + 2];
   }
 }

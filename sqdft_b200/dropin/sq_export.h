@@ -37,22 +37,26 @@ inline std::vector<double> block_field(double ***a, int nz, int ny, int nx, int 
 // order of ChargeDensity and ForcesLocal (type, main atom, replica): type,
 // global atom, coordinates and the intersection box; per type the radial
 // grid, rVloc, uu and their spline derivatives (getYD_gen, as both functions
-// form them) and the valence charge; rc_tilda; and the block fields as the
-// caller holds them: b, b_tilda, Vc, rho_at and phi with its FDn halo.
-inline void export_local(DS_SQ *p, CaseWriter &w) {
-  std::vector<int> rt, ra, box;
-  std::vector<double> xyz, Z;
+// form them) as 5 x size rows, and the valence charge.
+struct LocalInputs {
+  std::vector<int> rep_type, rep_atom, rep_box;
+  std::vector<double> rep_xyz, Z;
+  std::vector<std::vector<double>> tables;
+};
+
+inline LocalInputs gather_local(DS_SQ *p) {
+  LocalInputs L;
   int atom_count = 0;
   for (int t = 0; t < p->n_typ; t++) {
-    Z.push_back(p->Atm[t].Z);
+    L.Z.push_back(p->Atm[t].Z);
     for (int a = 0; a < p->Atm[t].natm; a++, atom_count++)
       for (int r = 0; r < p->Atm[t].Rx[a].n_replica; r++) {
         const DS_ProcAtm &X = p->Atm[t].Rx[a].ProcAtm[r], &Y = p->Atm[t].Ry[a].ProcAtm[r],
                          &W = p->Atm[t].Rz[a].ProcAtm[r];
-        rt.push_back(t);
-        ra.push_back(atom_count);
-        xyz.insert(xyz.end(), {X.coord, Y.coord, W.coord});
-        box.insert(box.end(), {X.start, X.end, Y.start, Y.end, W.start, W.end});
+        L.rep_type.push_back(t);
+        L.rep_atom.push_back(atom_count);
+        L.rep_xyz.insert(L.rep_xyz.end(), {X.coord, Y.coord, W.coord});
+        L.rep_box.insert(L.rep_box.end(), {X.start, X.end, Y.start, Y.end, W.start, W.end});
       }
     const int len = p->Psd[t].size;
     std::vector<double> tab((size_t)5 * len), dv(len), du(len);
@@ -65,14 +69,23 @@ inline void export_local(DS_SQ *p, CaseWriter &w) {
       tab[(size_t)3 * len + i] = p->Psd[t].uu[i];
       tab[(size_t)4 * len + i] = du[i];
     }
-    w.f64(("loc_tab" + std::to_string(t)).c_str(), tab.data(), {5, len});
+    L.tables.push_back(std::move(tab));
   }
-  const int64_t n = (int64_t)rt.size();
-  w.i32("loc_rep_type", rt.data(), {n});
-  w.i32("loc_rep_atom", ra.data(), {n});
-  w.f64("loc_rep_xyz", xyz.data(), {n, 3});
-  w.i32("loc_rep_box", box.data(), {n, 6});
-  w.f64("loc_Z", Z.data(), {p->n_typ});
+  return L;
+}
+
+// The pseudocharge inputs (gather_local) and rc_tilda, and the block fields
+// as the caller holds them: b, b_tilda, Vc, rho_at and phi with its FDn halo.
+inline void export_local(DS_SQ *p, CaseWriter &w) {
+  const LocalInputs L = gather_local(p);
+  for (int t = 0; t < p->n_typ; t++)
+    w.f64(("loc_tab" + std::to_string(t)).c_str(), L.tables[t].data(), {5, (int64_t)L.tables[t].size() / 5});
+  const int64_t n = (int64_t)L.rep_type.size();
+  w.i32("loc_rep_type", L.rep_type.data(), {n});
+  w.i32("loc_rep_atom", L.rep_atom.data(), {n});
+  w.f64("loc_rep_xyz", L.rep_xyz.data(), {n, 3});
+  w.i32("loc_rep_box", L.rep_box.data(), {n, 6});
+  w.f64("loc_Z", L.Z.data(), {p->n_typ});
   w.f64s("loc_rc_tilda", p->rc_tilda);
   const int nz = p->np_z, ny = p->np_y, nx = p->np_x, h = p->FDn;
   w.f64("loc_b", block_field(p->b, nz, ny, nx, 0).data(), {nz, ny, nx});

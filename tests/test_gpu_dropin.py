@@ -42,7 +42,7 @@ def test_golden_run_matches_published_log():
     assert g["fermi_iters"] == pub["fermi_iters"]
 
 
-def run_program(tmp_path: Path, precision: str | None = None, graph: int = 0) -> dict:
+def run_program(tmp_path: Path, precision: str | None = None, graph: int = 0, local: bool = False) -> dict:
     from sqdft_b200.configs.gen_configs import write_system
     from sqdft_b200.runlog import parse
 
@@ -56,6 +56,8 @@ def run_program(tmp_path: Path, precision: str | None = None, graph: int = 0) ->
         env["SQDFT_B200_PRECISION"] = precision
     if graph:
         env["SQDFT_B200_GRAPH"] = str(graph)
+    if local:
+        env["SQDFT_B200_LOCAL"] = "1"
     out = subprocess.run([str(PROGRAM), "-name", "al_ref"], cwd=run, env=env, capture_output=True, text=True,
                          timeout=900)
     (tmp_path / "sqdft_gpu.log").write_text(out.stdout + out.stderr)
@@ -102,6 +104,23 @@ def test_dropin_program_scf_loop_on_step_graphs(tmp_path):
     run, to the tolerances of the plain drop-in run."""
     g = json.loads(GOLDEN.read_text())
     got = run_program(tmp_path, graph=2)
+    assert len(got["scf"]) == len(g["scf"])
+    for a, b in zip(got["scf"], g["scf"]):
+        assert abs(a["fermi"] - b["fermi"]) <= 1e-9, (a, b)
+        assert abs(a["etot"] - b["etot"]) <= 1e-9, (a, b)
+    assert got["fermi_iters"] == g["fermi_iters"]
+    assert abs(got["free_energy"] - g["free_energy"]) <= 1e-8
+    assert np.abs(np.array(got["forces"]) - np.array(g["forces"])).max() <= 1e-7
+
+
+@pytest.mark.gpu
+def test_dropin_program_with_local_path_on_device(tmp_path):
+    """SQDFT_B200_LOCAL=1: ChargeDensity's per-atom loop and ForcesLocal run on
+    the GPU too (sqb_charge_density, sqb_forces_local), the rest of
+    ChargeDensity on the host.  The SCF history, free energy and forces match
+    the reference run to the tolerances of the plain drop-in run."""
+    g = json.loads(GOLDEN.read_text())
+    got = run_program(tmp_path, local=True)
     assert len(got["scf"]) == len(g["scf"])
     for a, b in zip(got["scf"], g["scf"]):
         assert abs(a["fermi"] - b["fermi"]) <= 1e-9, (a, b)
