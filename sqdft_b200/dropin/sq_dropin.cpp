@@ -55,13 +55,17 @@ int mpi_reduce(double *v, int count, int op, void *) {
   return MPI_Allreduce(MPI_IN_PLACE, v, count, MPI_DOUBLE, o, MPI_COMM_WORLD) == MPI_SUCCESS ? 0 : 1;
 }
 
+sqb_ctx *g_lctx = nullptr;  // the pseudocharge calls' context (SQDFT_B200_LOCAL=1)
+
 void destroy_ctx() {
   if (g_ctx) sqb_destroy(g_ctx);
   g_ctx = nullptr;
+  if (g_lctx) sqb_destroy(g_lctx);
+  g_lctx = nullptr;
 }
 
-void ensure_ctx(DS_SQ *p) {
-  if (g_ctx) return;
+// The block grid of DS_SQ (ds_sq.h:133-161) in the C-ABI layout.
+sqb_grid grid_of(DS_SQ *p) {
   sqb_grid g;
   std::memset(&g, 0, sizeof(g));
   g.np[0] = p->np_x;
@@ -84,11 +88,22 @@ void ensure_ctx(DS_SQ *p) {
     g.coeff_lap[k] = p->coeff_lap[k];
     g.coeff_grad[k] = p->coeff_grad[k];
   }
+  return g;
+}
+
+int device_of() {
   int rank = 0;
   MPI_Comm_rank(MPI_COMM_WORLD, &rank);
   const char *dev_env = std::getenv("SQDFT_B200_DEVICE");
-  const int device = dev_env ? std::atoi(dev_env) : rank;
-  int rc = sqb_create(&g, device, &g_ctx);
+  return dev_env ? std::atoi(dev_env) : rank;
+}
+
+// The SQ context: created at the first SQ call, when DS_SQ::Ncharge (the
+// electron count the Fermi level is solved for) is set.
+void ensure_ctx(DS_SQ *p) {
+  if (g_ctx) return;
+  const sqb_grid g = grid_of(p);
+  int rc = sqb_create(&g, device_of(), &g_ctx);
   if (rc) fail(rc, "sqb_create");
   const char *prec = std::getenv("SQDFT_B200_PRECISION");
   if (prec && (!std::strcmp(prec, "fp32") || !std::strcmp(prec, "mixed"))) sqb_set_precision(g_ctx, SQB_FP32_MIXED);
@@ -294,7 +309,19 @@ bool local_on_device() {
   return v && !std::strcmp(v, "1") && !export_mode();
 }
 
+// The pseudocharge calls run on a context of their own: ChargeDensity comes
+// before the SQ context can be made (it sets the electron count).
+void ensure_local_ctx(DS_SQ *p) {
+  if (g_lctx) return;
+  const sqb_grid g = grid_of(p);
+  int rc = sqb_create(&g, device_of(), &g_lctx);
+  if (rc) fail(rc, "sqb_create");
+  if (p->nproc > 1) sqb_set_allreduce(g_lctx, mpi_reduce, nullptr);
+  std::atexit(destroy_ctx);
+}
+
 void upload_local_atoms(DS_SQ *p) {
+  ensure_local_ctx(p);
   const sqb::LocalInputs L = sqb::gather_local(p);
   std::vector<sqb_local_species> sp(p->n_typ);
   for (int t = 0; t < p->n_typ; t++) {
@@ -302,7 +329,7 @@ void upload_local_atoms(DS_SQ *p) {
     sp[t].Z = L.Z[t];
     sp[t].tables = L.tables[t].data();
   }
-  const int rc = sqb_set_local_atoms(g_ctx, p->n_typ, sp.data(), (int)L.rep_type.size(), L.rep_type.data(),
+  const int rc = sqb_set_local_atoms(g_lctx, p->n_typ, sp.data(), (int)L.rep_type.size(), L.rep_type.data(),
                                      L.rep_atom.data(), L.rep_xyz.data(), L.rep_box.data(), p->rc_tilda, p->n_atm);
   if (rc) fail(rc, "local atoms");
 }
@@ -321,14 +348,13 @@ void ChargeDensity(DS_SQ *p) {
   }
   int rank = 0;
   MPI_Comm_rank(MPI_COMM_WORLD, &rank);
-  ensure_ctx(p);
   p->rc_tilda = 0.5;  // initialize.cpp:483
   upload_local_atoms(p);
   const int nz = p->np_z, ny = p->np_y, nx = p->np_x;
   const size_t N = (size_t)nz * ny * nx;
   std::vector<double> b(N), bt(N), vc(N), ra(N);
   double scal[7];
-  int rc = sqb_charge_density(g_ctx, b.data(), bt.data(), vc.data(), ra.data(), scal);
+  int rc = sqb_charge_density(g_lctx, b.data(), bt.data(), vc.data(), ra.data(), scal);
   if (rc) fail(rc, "ChargeDensity");
   // b, the scaled b_tilda and the shifted Vc replace the block's; rho_at
   // accumulates as the reference's loop adds into it (initialize.cpp:585)
@@ -383,14 +409,13 @@ void ForcesLocal(DS_SQ *p) {
     ref_ForcesLocal(p);
     return;
   }
-  ensure_ctx(p);
   upload_local_atoms(p);
   const int nz = p->np_z, ny = p->np_y, nx = p->np_x;
   const std::vector<double> phi = sqb::block_field(p->phi, nz, ny, nx, p->FDn);
   const std::vector<double> vc = sqb::block_field(p->Vc, nz, ny, nx, 0), b = sqb::block_field(p->b, nz, ny, nx, 0),
                             bt = sqb::block_field(p->b_tilda, nz, ny, nx, 0);
   std::vector<double> fl((size_t)3 * p->n_atm), fc((size_t)3 * p->n_atm);
-  const int rc = sqb_forces_local(g_ctx, phi.data(), vc.data(), b.data(), bt.data(), fl.data(), fc.data());
+  const int rc = sqb_forces_local(g_lctx, phi.data(), vc.data(), b.data(), bt.data(), fl.data(), fc.data());
   if (rc) fail(rc, "ForcesLocal");
   for (int a = 0; a < p->n_atm; a++) {
     p->flocx[a] = fl[3 * a];
