@@ -139,3 +139,80 @@ def test_block_split_in_two_matches_the_whole():
         assert abs(sum(p[key] for p in parts) - whole[key]) <= 1e-12 * abs(whole[key]), key
     for q in range(2):
         assert np.abs(forces[0][q] + forces[1][q] - fw[q]).max() <= 1e-12
+
+
+def _slab(grid, loc, z0, z1):
+    """The block's z-slab [z0, z1) with its replicas' boxes clipped to it
+    (what Replica_atoms gives the rank that holds the slab)."""
+    import dataclasses
+
+    g = dataclasses.replace(grid, np_=(grid.np_[0], grid.np_[1], z1 - z0),
+                            pnode_s=(grid.pnode_s[0], grid.pnode_s[1], grid.pnode_s[2] + z0))
+    box = loc.rep_box.copy()
+    lo, hi = g.pnode_s[2], g.pnode_s[2] + g.np_[2] - 1
+    keep = (box[:, 5] >= lo) & (box[:, 4] <= hi)
+    box[:, 4] = np.maximum(box[:, 4], lo)
+    box[:, 5] = np.minimum(box[:, 5], hi)
+    sub = dataclasses.replace(loc, rep_type=loc.rep_type[keep], rep_atom=loc.rep_atom[keep],
+                              rep_xyz=loc.rep_xyz[keep], rep_box=np.ascontiguousarray(box[keep]))
+    return g, sub
+
+
+def _rank_worker(rank: int, world: int, init_file: str, out_dir: str) -> None:
+    import datetime
+    import os
+    import sys
+
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    import torch.distributed as dist
+
+    from sqdft_b200 import sq
+    from sqdft_b200.dist import allreduce_fn
+    from test_gpu_local import _fixture, _slab
+
+    dist.init_process_group("gloo", init_method=f"file://{init_file}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        grid, loc, _, _ = _fixture("lihs")
+        cut = grid.np_[2] // 2
+        z0, z1 = (0, cut) if rank == 0 else (cut, grid.np_[2])
+        g, sub = _slab(grid, loc, z0, z1)
+        with sq.LocalContext(g, sub, allreduce=allreduce_fn(dist)) as ctx:
+            out = ctx.charge_density()
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), **{k: np.asarray(v) for k, v in out.items()})
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_through_the_allreduce_hook():
+    """Two gloo ranks on one GPU, each with its z-slab of the LiH block: the
+    sums go through sqb_set_allreduce (the reference's MPI_Allreduce of
+    initialize.cpp:717-723 and 770), V000 and Vcon come from the rank whose
+    block starts the main domain.  b and rho_at are the single-rank slices
+    bit for bit; the scaled b_tilda, the shifted Vc, Eself, Ncharge and Ecorr
+    agree with the single-rank call to rounding.  The ranks' kernels never
+    wait on each other: every exchange goes through the host."""
+    import os
+    import tempfile
+
+    import torch.multiprocessing as mp
+
+    from sqdft_b200 import sq
+
+    grid, loc, _, _ = _fixture("lihs")
+    with sq.LocalContext(grid, loc) as ctx:
+        whole = ctx.charge_density()
+    with tempfile.TemporaryDirectory() as td:
+        mp.start_processes(_rank_worker, args=(2, os.path.join(td, "init"), td), nprocs=2, start_method="spawn",
+                           join=True)
+        parts = [dict(np.load(os.path.join(td, f"rank{r}.npz"))) for r in range(2)]
+    for key in ("b", "rho_at"):
+        assert np.array_equal(np.concatenate([p[key] for p in parts]), whole[key]), key
+    for key in ("b_tilda", "vc"):
+        assert _rel(np.concatenate([p[key] for p in parts]), whole[key]) <= 1e-13, key
+    for p in parts:
+        for key in ("Eself", "Ncharge", "Ncharge_tilda", "Eself_tilda"):
+            assert abs(float(p[key]) - whole[key]) <= 1e-12 * abs(whole[key]), key
+        assert abs(float(p["Ecorr"]) - whole["Ecorr"]) <= _ecorr_tol(whole)
+        assert float(p["Vcon"]) == whole["Vcon"]
