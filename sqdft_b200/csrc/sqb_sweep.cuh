@@ -14,6 +14,10 @@
 //   * the 2 FDN + 1 planes of a column's stencil: the centre and the FDN
 //     planes ahead in registers, the FDN planes behind in the thread's own
 //     slots of a shared ring (no barrier: no other thread reads them);
+//   * the shared planes rotate through three buffers under a split barrier:
+//     a thread writes plane z + 1 and arrives on an mbarrier before it works
+//     on plane z, and waits for that phase (bounded) only afterwards, so
+//     warps drift by up to a plane instead of meeting at every plane;
 //   * the nonlocal term reads the layered projector fields (sqb_internal.cuh):
 //     per point and layer one 16-bit projector base and the projector values,
 //     so the gather sum_J c_J chi_J(x) is a fixed loop over four layers with
