@@ -568,11 +568,42 @@ def run_ours(args):
         if cpu:
             res["cpu_baseline"] = cpu
     ctx.close()
+    if res and ws == 1:
+        res["pseudocharge"] = pseudocharge_timing(args.config)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
     if res:
         print(json.dumps(res), flush=True)
+
+
+def pseudocharge_timing(config: str, steps: int = 2) -> dict:
+    """Device time of one sqb_charge_density and one sqb_forces_local (the
+    per-atom loops of ChargeDensity and ForcesLocal) on the configuration,
+    after one untimed call; reported beside the SQ step, outside its timed
+    region."""
+    try:
+        from sqdft_b200 import sq
+        from sqdft_b200.case import read_container
+        from sqdft_b200.cases import make_case
+        from sqdft_b200.pseudocharge import fields_from_arrays, grid_from_arrays, local_from_arrays
+
+        a = read_container(make_case(config))
+        grid, loc, f = grid_from_arrays(a), local_from_arrays(a), fields_from_arrays(a)
+        cd, fl = [], []
+        with sq.LocalContext(grid, loc) as lctx:
+            for it in range(steps + 1):
+                out = lctx.charge_density()
+                lctx.forces_local(f["phi"], f["vc"], f["b"], f["b_tilda"])
+                if it:
+                    st = lctx.stats()
+                    cd.append(st["ms_charge_density"])
+                    fl.append(st["ms_forces_local"])
+        ms = float(np.mean(cd) + np.mean(fl))
+        return {"replicas": loc.n_rep, "charge_density_ms": float(np.mean(cd)), "forces_local_ms": float(np.mean(fl)),
+                "replicas_per_s": loc.n_rep / (ms * 1e-3), "b_matches_reference_export": bool(np.array_equal(out["b"], f["b"]))}
+    except Exception as e:  # reported, never fatal for the SQ line
+        return {"unavailable": f"{type(e).__name__}: {e}"[:200]}
 
 
 def reference_rate(config: str, sample: int, threads: int):
