@@ -216,3 +216,38 @@ def test_two_ranks_through_the_allreduce_hook():
             assert abs(float(p[key]) - whole[key]) <= 1e-12 * abs(whole[key]), key
         assert abs(float(p["Ecorr"]) - whole["Ecorr"]) <= _ecorr_tol(whole)
         assert float(p["Vcon"]) == whole["Vcon"]
+
+
+def test_argument_and_state_errors():
+    """A replica box outside the block is rejected on the host (SQB_ERR_ARG)
+    before anything runs, and the pseudocharge calls before
+    sqb_set_local_atoms return SQB_ERR_STATE."""
+    import ctypes
+    import dataclasses
+
+    from sqdft_b200 import sq
+
+    grid, loc, f, _ = _fixture("tiny")
+    bad = loc.rep_box.copy()
+    bad[0, 1] = grid.pnode_s[0] + grid.np_[0]  # one node past the block
+    with pytest.raises(sq.SQBError) as err:
+        sq.LocalContext(grid, dataclasses.replace(loc, rep_box=bad))
+    assert err.value.code == 1
+    with sq.LocalContext(grid, loc) as ctx:
+        # a second context of the same grid, without replicas
+        g = sq.SqbGrid()
+        g.np[:] = list(grid.np_)
+        g.pnode_s[:] = list(grid.pnode_s)
+        g.n_int[:] = list(grid.np_)
+        g.nloc, g.fdn, g.npl, g.fermi_alg = 1, grid.fdn, 4, 1
+        g.delta, g.bet = grid.delta, 1.0
+        ptr = ctypes.c_void_p()
+        assert ctx.lib.sqb_create(ctypes.byref(g), 0, ctypes.byref(ptr)) == 0
+        try:
+            scal = np.zeros(7)
+            assert ctx.lib.sqb_charge_density(ptr, None, None, None, None, sq._d(scal)) == 12  # SQB_ERR_STATE
+            out = np.zeros((grid.n_atm, 3))
+            args = [np.ascontiguousarray(f[k]) for k in ("phi", "vc", "b", "b_tilda")]
+            assert ctx.lib.sqb_forces_local(ptr, *[sq._d(x) for x in args], sq._d(out), sq._d(out)) == 12
+        finally:
+            ctx.lib.sqb_destroy(ptr)
