@@ -54,3 +54,25 @@ def test_forces_local_matches_reference(name):
     assert np.abs(floc - a["fl_floc"]).max() <= 1e-12
     assert np.abs(fcorr - a["fl_fcorr"]).max() <= 1e-12
     assert np.abs(a["fl_floc"]).max() > 1e-6  # the fixture holds real forces
+
+
+@pytest.mark.parametrize("config", ["c1", "c2"])
+def test_charge_density_matches_reference_on_configurations(config):
+    """The benchmark configurations' case files hold the reference's own
+    ChargeDensity output (the drop-in program's export runs the reference
+    function): the restatement reproduces b, b_tilda, Vc and rho_at of c1
+    (4 atoms, 16^3 grid) and c2 (108 atoms, 48^3 grid, 364 replicas)."""
+    from oracle.pyoracle import LocalOracle
+    from sqdft_b200.case import read_container
+    from sqdft_b200.cases import case_path
+    from sqdft_b200.pseudocharge import grid_from_arrays, local_from_arrays
+
+    path = case_path(config)
+    if not path.exists():
+        pytest.skip(f"case file not built: {path}")
+    a = read_container(path)
+    if "loc_b" not in a:
+        pytest.skip("case file exported without the pseudocharge data")
+    out = LocalOracle(grid_from_arrays(a), local_from_arrays(a)).charge_density()
+    for key in ("b", "b_tilda", "vc", "rho_at"):
+        assert _close(out[key], a[f"loc_{key}"], 1e-14), key
