@@ -17,7 +17,9 @@
 //   --local          also write <out_prefix>_local.sqc: the pseudocharge
 //                    replicas and radial tables, ChargeDensity's outputs
 //                    (initialize.cpp:470-784) as the call leaves them, and
-//                    ForcesLocal (forces.cpp:20-315) with the fields it read
+//                    ForcesLocal (forces.cpp:20-315) with the fields it read,
+//                    with the time of both calls (with --nodes-only: before
+//                    the SQ step, on the set-up's phi)
 //   --sample K       CPU baseline: time the reference's per-node work
 //                    (LanczosAlgorithm, sq.cpp:965, and the moment loop of
 //                    sq.cpp:564-655 over HsubTimesVec) on K nodes spread over
@@ -241,9 +243,43 @@ int main(int argc, char **argv) {
     return 0;
   }
 
+  // --local: the pseudocharge inputs, ChargeDensity's outputs as the call
+  // left them, and ForcesLocal with the fields it reads (phi, Vc, b, b_tilda)
+  auto write_local = [&]() {
+    sqb::CaseWriter wl(out + "_local.sqc");
+    // the pseudocharge inputs and the fields ForcesLocal reads (phi, Vc, b, b_tilda)
+    sqb::export_local(&SQ, wl);
+    const int nz = SQ.np_z, ny = SQ.np_y, nx = SQ.np_x;
+    wl.f64("cd_b", cd_b.data(), {nz, ny, nx});
+    wl.f64("cd_b_tilda", cd_bt.data(), {nz, ny, nx});
+    wl.f64("cd_vc", cd_vc.data(), {nz, ny, nx});
+    wl.f64("cd_rho_at", cd_rho_at.data(), {nz, ny, nx});
+    wl.f64s("cd_Eself", SQ.Eself);
+    wl.f64s("cd_Ncharge", SQ.Ncharge);
+    wl.f64s("cd_Ecorr", SQ.Ecorr);
+    wl.f64s("t_charge_density", t_cd);
+    t0 = MPI_Wtime();
+    ForcesLocal(&SQ);
+    const double t_fl = MPI_Wtime() - t0;
+    std::vector<double> fl((size_t)SQ.n_atm * 3), fc((size_t)SQ.n_atm * 3);
+    for (int a = 0; a < SQ.n_atm; a++) {
+      fl[3 * a] = SQ.flocx[a];
+      fl[3 * a + 1] = SQ.flocy[a];
+      fl[3 * a + 2] = SQ.flocz[a];
+      fc[3 * a] = SQ.fcorrx[a];
+      fc[3 * a + 1] = SQ.fcorry[a];
+      fc[3 * a + 2] = SQ.fcorrz[a];
+    }
+    wl.f64("fl_floc", fl.data(), {SQ.n_atm, 3});
+    wl.f64("fl_fcorr", fc.data(), {SQ.n_atm, 3});
+    wl.f64s("t_forces_local", t_fl);
+    wl.close();
+  };
+
   if (nodes_only) {
     // Only the block interior is valid here; the SQ call fills the halo.
     sqb::export_case(&SQ, (out + "_in.sqc").c_str(), scf_iter, true);
+    if (do_local) write_local();  // phi is the set-up's Poisson solution; no SQ step needed
     return 0;
   }
 
@@ -328,36 +364,7 @@ int main(int argc, char **argv) {
   }
   w.close();
 
-  if (do_local) {
-    sqb::CaseWriter wl(out + "_local.sqc");
-    // the pseudocharge inputs and the fields ForcesLocal reads (phi, Vc, b, b_tilda)
-    sqb::export_local(&SQ, wl);
-    const int nz = SQ.np_z, ny = SQ.np_y, nx = SQ.np_x;
-    wl.f64("cd_b", cd_b.data(), {nz, ny, nx});
-    wl.f64("cd_b_tilda", cd_bt.data(), {nz, ny, nx});
-    wl.f64("cd_vc", cd_vc.data(), {nz, ny, nx});
-    wl.f64("cd_rho_at", cd_rho_at.data(), {nz, ny, nx});
-    wl.f64s("cd_Eself", SQ.Eself);
-    wl.f64s("cd_Ncharge", SQ.Ncharge);
-    wl.f64s("cd_Ecorr", SQ.Ecorr);
-    wl.f64s("t_charge_density", t_cd);
-    t0 = MPI_Wtime();
-    ForcesLocal(&SQ);
-    const double t_fl = MPI_Wtime() - t0;
-    std::vector<double> fl((size_t)SQ.n_atm * 3), fc((size_t)SQ.n_atm * 3);
-    for (int a = 0; a < SQ.n_atm; a++) {
-      fl[3 * a] = SQ.flocx[a];
-      fl[3 * a + 1] = SQ.flocy[a];
-      fl[3 * a + 2] = SQ.flocz[a];
-      fc[3 * a] = SQ.fcorrx[a];
-      fc[3 * a + 1] = SQ.fcorry[a];
-      fc[3 * a + 2] = SQ.fcorrz[a];
-    }
-    wl.f64("fl_floc", fl.data(), {SQ.n_atm, 3});
-    wl.f64("fl_fcorr", fc.data(), {SQ.n_atm, 3});
-    wl.f64s("t_forces_local", t_fl);
-    wl.close();
-  }
+  if (do_local) write_local();
   std::printf("sqref_driver: wrote %s_in.sqc and %s_out.sqc (SQ %.3f s)\n", out.c_str(), out.c_str(), t_sq);
   return 0;
 }
