@@ -14,6 +14,7 @@ mode and the fixtures of tests/golden carry them as ``loc_*`` arrays.
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
 
 import numpy as np
@@ -70,3 +71,72 @@ def fields_from_arrays(a: dict) -> dict:
     """The block fields a container holds for ForcesLocal: phi (with its FDn
     halo), Vc, b, b_tilda."""
     return {k: np.asarray(a[f"loc_{k}"], np.float64) for k in ("phi", "vc", "b", "b_tilda")}
+
+
+_TEMP_TOL = 1e-12  # TEMP_TOL of the reference
+
+
+def _c_round(x: float) -> int:
+    """C's round(): to nearest, halves away from zero (exact for |x| < 2^52)."""
+    a = abs(x)
+    f = math.floor(a)
+    r = f + (1 if a - f >= 0.5 else 0)
+    return int(r) if x >= 0 else -int(r)
+
+
+def pseudocharge_replicas(atoms_xyz, atom_type, rb, domain, n_int, pnode_s, np_):
+    """Replica_atoms (initialize.cpp:21-160): every periodic image of every
+    atom whose rb-box, centred on the image's nearest grid node, meets the
+    block [pnode_s, pnode_s + np_), with the intersection box.
+
+    ``atoms_xyz`` [n_atm, 3] are the main-domain positions (DS_coord::main_atm)
+    in type-major order with types ``atom_type``; ``rb`` the per-type cutoffs
+    as the .atoms file gives them (rounded up to a multiple of the mesh size
+    here, readfiles.cpp:513); ``domain`` the three domain lengths of the
+    .input file.  Returns (rep_type, rep_atom, rep_xyz, rep_box) in the
+    reference's loop order (type, main atom, image z-y-x), as
+    :class:`LocalAtoms` holds them."""
+    domain = [float(d) for d in domain]
+    delta = domain[0] / int(n_int[0])  # readfiles.cpp:294-303
+    rb_eff = [math.ceil(r / delta) * delta for r in rb]
+    ps = [int(p) for p in pnode_s]
+    pe = [int(pnode_s[d]) + int(np_[d]) - 1 for d in range(3)]
+    xyz = np.asarray(atoms_xyz, np.float64).reshape(-1, 3)
+    types = np.asarray(atom_type, np.int64).reshape(-1)
+    rt, ra, rx, rbox = [], [], [], []
+
+    def nearest(c):
+        n = _c_round(c / delta)
+        if abs(abs(n * delta - c) - delta * 0.5) < _TEMP_TOL:
+            n = math.floor((c / delta) - 10 * _TEMP_TOL)
+        return n
+
+    def overlap(lo, hi, s, e):
+        start = lo if s <= lo <= e else (s if lo <= s <= hi else -1)
+        end = hi if s <= hi <= e else (e if lo <= e <= hi else -1)
+        return start, end
+
+    atom = 0
+    for t in range(len(rb)):
+        r_b = rb_eff[t]
+        half = _c_round(r_b / delta)
+        for a in np.nonzero(types == t)[0]:
+            c = xyz[a]
+            hi = [math.floor(((domain[d] + r_b - c[d]) / domain[d]) + _TEMP_TOL) for d in range(3)]
+            lo = [math.ceil(((-r_b - c[d]) / domain[d]) - _TEMP_TOL) for d in range(3)]
+            for rr in range(lo[2], hi[2] + 1):
+                for qq in range(lo[1], hi[1] + 1):
+                    for pp in range(lo[0], hi[0] + 1):
+                        img = (c[0] + pp * domain[0], c[1] + qq * domain[1], c[2] + rr * domain[2])
+                        box = []
+                        for d in range(3):
+                            n = nearest(img[d])
+                            box.extend(overlap(n - half, n + half, ps[d], pe[d]))
+                        if -1 not in box:
+                            rt.append(t)
+                            ra.append(atom)
+                            rx.append(img)
+                            rbox.append(box)
+            atom += 1
+    return (np.array(rt, np.int32), np.array(ra, np.int32), np.array(rx, np.float64).reshape(-1, 3),
+            np.array(rbox, np.int32).reshape(-1, 6))

@@ -76,3 +76,34 @@ def test_charge_density_matches_reference_on_configurations(config):
     out = LocalOracle(grid_from_arrays(a), local_from_arrays(a)).charge_density()
     for key in ("b", "b_tilda", "vc", "rho_at"):
         assert _close(out[key], a[f"loc_{key}"], 1e-14), key
+
+
+@pytest.mark.parametrize("name", ["tiny", "lihs", "c1", "c2", "c5"])
+def test_pseudocharge_replicas_match_reference(name):
+    """sqdft_b200.pseudocharge.pseudocharge_replicas restates Replica_atoms
+    (initialize.cpp:21-160): from the main-domain positions, the .atoms
+    cutoffs rb and the .input domain it gives the reference's own replica
+    list (exported by the drop-in program from DS_coord::ProcAtm) exactly:
+    types, atoms, image coordinates and intersection boxes."""
+    from sqdft_b200.case import read_container
+    from sqdft_b200.cases import case_path
+    from sqdft_b200.configs.gen_configs import SPECIES, SYSTEMS, positions
+    from sqdft_b200.pseudocharge import grid_from_arrays, local_from_arrays, pseudocharge_replicas
+
+    path = case_path(name)
+    if not path.exists():
+        pytest.skip(f"case file not built: {path}")
+    a = read_container(path)
+    if "loc_rep_box" not in a:
+        pytest.skip("case file exported without the pseudocharge data")
+    s = SYSTEMS[name]
+    rb = [SPECIES[sym][4] for sym in positions(s)]
+    domain = [float(f"{s.domain:.10f}")] * 3  # as the .input file writes it
+    grid, loc = grid_from_arrays(a), local_from_arrays(a)
+    n_int = a["params_i"][0:3]
+    rt, ra, rx, box = pseudocharge_replicas(a["atoms_xyz"], a["atom_type"], rb, domain, n_int, grid.pnode_s,
+                                            grid.np_)
+    assert np.array_equal(rt, loc.rep_type)
+    assert np.array_equal(ra, loc.rep_atom)
+    assert np.array_equal(rx, loc.rep_xyz)
+    assert np.array_equal(box, loc.rep_box)
