@@ -140,3 +140,51 @@ def pseudocharge_replicas(atoms_xyz, atom_type, rb, domain, n_int, pnode_s, np_)
             atom += 1
     return (np.array(rt, np.int32), np.array(ra, np.int32), np.array(rx, np.float64).reshape(-1, 3),
             np.array(rbox, np.int32).reshape(-1, 6))
+
+
+def projector_replicas(atoms_xyz, atom_type, rc, domain, n_int, pnode_s, np_, nloc):
+    """Replica_atoms_Rcut (initialize.cpp:1003-1196): every periodic image of
+    every atom whose rc-box, centred on the image's nearest grid node, meets
+    the block widened by the truncation half-width nloc on every side -- the
+    replicas whose projectors the SQ windows of the block can see
+    (sqb_set_atoms).  ``rc`` are the per-type projector radii as DS_Psd holds
+    them (the case container's ``typ_d[:, 0]``), Rcut = nloc * delta
+    (readfiles.cpp:306-307).  Returns (rep_type, rep_atom, rep_xyz) in the
+    reference's loop order."""
+    domain = [float(d) for d in domain]
+    delta = domain[0] / int(n_int[0])
+    rcut = nloc * delta
+    ps = [int(pnode_s[d]) - nloc for d in range(3)]
+    pe = [int(pnode_s[d]) + int(np_[d]) - 1 + nloc for d in range(3)]
+    xyz = np.asarray(atoms_xyz, np.float64).reshape(-1, 3)
+    types = np.asarray(atom_type, np.int64).reshape(-1)
+    rt, ra, rx = [], [], []
+
+    def nearest(c):
+        n = _c_round(c / delta)
+        if abs(abs(n * delta - c) - delta * 0.5) < _TEMP_TOL:
+            n = math.floor((c / delta) - 10 * _TEMP_TOL)
+        return n
+
+    def meets(lo, hi, s, e):
+        start = s <= lo <= e or lo <= s <= hi
+        end = s <= hi <= e or lo <= e <= hi
+        return start and end
+
+    atom = 0
+    for t in range(len(rc)):
+        half = math.ceil(rc[t] / delta)
+        for a in np.nonzero(types == t)[0]:
+            c = xyz[a]
+            hi = [math.floor(((domain[d] + rcut + rc[t] - c[d]) / domain[d]) + _TEMP_TOL) for d in range(3)]
+            lo = [math.ceil(((-(rcut + rc[t]) - c[d]) / domain[d]) - _TEMP_TOL) for d in range(3)]
+            for rr in range(lo[2], hi[2] + 1):
+                for qq in range(lo[1], hi[1] + 1):
+                    for pp in range(lo[0], hi[0] + 1):
+                        img = (c[0] + pp * domain[0], c[1] + qq * domain[1], c[2] + rr * domain[2])
+                        if all(meets(nearest(img[d]) - half, nearest(img[d]) + half, ps[d], pe[d]) for d in range(3)):
+                            rt.append(t)
+                            ra.append(atom)
+                            rx.append(img)
+            atom += 1
+    return np.array(rt, np.int32), np.array(ra, np.int32), np.array(rx, np.float64).reshape(-1, 3)

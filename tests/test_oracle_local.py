@@ -107,3 +107,26 @@ def test_pseudocharge_replicas_match_reference(name):
     assert np.array_equal(ra, loc.rep_atom)
     assert np.array_equal(rx, loc.rep_xyz)
     assert np.array_equal(box, loc.rep_box)
+
+
+@pytest.mark.parametrize("name", ["tiny", "lihs", "c1", "c2", "c3", "c5"])
+def test_projector_replicas_match_reference(name):
+    """sqdft_b200.pseudocharge.projector_replicas restates Replica_atoms_Rcut
+    (initialize.cpp:1003-1196) and gives the replica list of the SQ step
+    (sqb_set_atoms) that the reference built, exactly."""
+    from sqdft_b200.case import read_container
+    from sqdft_b200.cases import case_path
+    from sqdft_b200.configs.gen_configs import SYSTEMS
+    from sqdft_b200.pseudocharge import projector_replicas
+
+    path = case_path(name)
+    if not path.exists():
+        pytest.skip(f"case file not built: {path}")
+    a = read_container(path)
+    s = SYSTEMS[name]
+    pi = a["params_i"]
+    rt, ra, rx = projector_replicas(a["atoms_xyz"], a["atom_type"], a["typ_d"][:, 0], [float(f"{s.domain:.10f}")] * 3,
+                                    pi[0:3], pi[6:9], pi[3:6], int(pi[9]))
+    assert np.array_equal(rt, a["rep_i"][:, 0])
+    assert np.array_equal(ra, a["rep_i"][:, 2])
+    assert np.array_equal(rx, a["rep_xyz"])
